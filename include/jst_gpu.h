@@ -1,0 +1,196 @@
+/*
+ * jst_gpu.h — C ABI of the B200 (sm_100a) implementation of PurineCFD's
+ * explicit JST + Spalart-Allmaras RANS loop (the jst-rs `Solver`).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns a jst_status.  Each handle is single-threaded (like the reference's
+ * `&mut Solver`); separate handles may be used from separate threads.  All
+ * cell arrays crossing the boundary are the interior NI x NJ cells, i-major /
+ * j-minor (the order of the reference's golden data and `result.csv`), where
+ * i is the radial ring index (0 = wall) and j the circumferential index.
+ *
+ * Citations are file:line in the reference's jst-rs crate; each entry point
+ * names the Rust interface it replaces.
+ */
+#ifndef JST_GPU_H
+#define JST_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct jst_solver jst_solver;
+
+/* Status codes.  The JST_ERR_MESH_* values map one-to-one onto the
+ * reference's MeshError variants (mesh.rs:17-44); JST_ERR_CONFIG is its
+ * io::Error(InvalidData) from Config::from_str (config.rs:243-248);
+ * JST_ERR_NONPHYSICAL is NonPhysical (state.rs:589-606). */
+typedef enum {
+    JST_OK = 0,
+    JST_ERR_MESH_IO = 1,
+    JST_ERR_MESH_BAD_HEADER = 2,
+    JST_ERR_MESH_EMPTY = 3,
+    JST_ERR_MESH_COUNT_MISMATCH = 4,
+    JST_ERR_MESH_BAD_POINT = 5,
+    JST_ERR_MESH_TOO_SMALL = 6,
+    JST_ERR_CONFIG = 7,
+    JST_ERR_NONPHYSICAL = 8,
+    JST_ERR_CUDA = 9,
+    JST_ERR_TIMEOUT = 10,
+    JST_ERR_OOM = 11,
+    JST_ERR_ARG = 12
+} jst_status;
+
+/* Arithmetic of the stage kernels. */
+typedef enum {
+    JST_PREC_FP64 = 0,      /* everything in FP64 (the reference's arithmetic) */
+    JST_PREC_FP32_SPLIT = 1 /* FP32 fluxes/dissipation/gradients/SA; FP64 metrics,
+                               wall distance, U_n accumulator, reductions */
+} jst_precision;
+
+/* Time step used by the RK update. */
+typedef enum {
+    JST_DT_GLOBAL = 0, /* every cell advances with the global minimum step (solver.rs:110-116) */
+    JST_DT_LOCAL = 1   /* each cell advances with its own CFL step (steady-state acceleration) */
+} jst_dt_mode;
+
+/* Which kernels run a stage. */
+typedef enum {
+    JST_PATH_FUSED = 0, /* one tiled kernel per RK stage (production) */
+    JST_PATH_PASSES = 1 /* one kernel per reference pass, strict FP64 (parity mode) */
+} jst_kernel_path;
+
+typedef struct {
+    int precision;   /* jst_precision */
+    int dt_mode;     /* jst_dt_mode */
+    int kernel_path; /* jst_kernel_path */
+    int device;      /* CUDA device ordinal */
+    int tile_i;      /* fused path tile rows (0 = autotuned) */
+    int tile_j;      /* fused path tile columns (0 = autotuned) */
+    int use_graph;   /* capture each RK step as a CUDA graph (fused path) */
+    double nut_inf_ratio; /* free-stream nu-tilde / nu; <= 0 uses the config value or 0.1 */
+} jst_opts;
+
+/* Fills opts with the defaults: FP64, global dt, fused path, device 0,
+ * autotuned tiles, graphs on, nu-tilde ratio from the config. */
+void jst_default_opts(jst_opts* opts);
+
+/* Solver::from_paths (solver.rs:64-68): read config.json and an O-mesh text
+ * file, build geometry, initialise the free stream and apply the boundary
+ * conditions (Solver::new, solver.rs:47-62). */
+jst_status jst_create_from_paths(const char* config_path, const char* mesh_path, const jst_opts* opts,
+                                 jst_solver** out);
+
+/* Solver::new (solver.rs:47-62) from a config.json text and a node array
+ * (n_rings x n_theta nodes, (x, y) interleaved, ring-major, counter-clockwise;
+ * a closing duplicate point per ring is trimmed as in mesh.rs:169-189). */
+jst_status jst_create(const char* config_json, const double* xy, int n_rings, int n_theta, const jst_opts* opts,
+                      jst_solver** out);
+
+/* Releases the handle and its device memory. */
+void jst_destroy(jst_solver* s);
+
+/* Message of the last error on this handle (or of the last failed create
+ * when s is NULL). */
+const char* jst_last_error(const jst_solver* s);
+
+/* Mesh sizes: NI = n_rings - 1 radial cells, NJ circumferential cells. */
+int jst_ni(const jst_solver* s);
+int jst_nj(const jst_solver* s);
+
+/* The NonPhysical error of state.rs:589-606. */
+typedef struct {
+    int64_t i, j;
+    double rho, p;
+} jst_nonphysical;
+
+/* Solver::advance (solver.rs:97-120): one 5-stage RK step.  On
+ * JST_ERR_NONPHYSICAL the first offending cell (row-major order within the
+ * first failing stage) is written to *bad (may be NULL). */
+jst_status jst_advance(jst_solver* s, jst_nonphysical* bad);
+
+/* RunReport (solver.rs:36-43). */
+typedef struct {
+    int64_t steps;
+    double residual;
+    double totaltime;
+    int converged;
+} jst_run_report;
+
+typedef void (*jst_step_cb)(void* user, uint64_t step, double residual);
+
+/* Solver::run (solver.rs:203-226): advance until max_steps (< 0: the config's
+ * solver.iteration) or until the residual drops below solver.targetres.  The
+ * callback (may be NULL) runs on the caller's thread after each step with the
+ * step's residual (solver.rs:190-200). */
+jst_status jst_run(jst_solver* s, int64_t max_steps, jst_step_cb cb, void* user, jst_run_report* report,
+                   jst_nonphysical* bad);
+
+/* Solver::residual_terms (solver.rs:86-94): boundary conditions plus the
+ * residual terms Fc, Fv, Fd, S of the current state, without an update
+ * (golden/bench use).  Also computes the per-cell local time step first
+ * when *dt is non-NULL (timestep::compute, timestep.rs:24-47), returning the
+ * global minimum in *dt. */
+jst_status jst_residual_terms(jst_solver* s, double* dt);
+
+/* timestep::compute (timestep.rs:24-57) on the current state. */
+jst_status jst_timestep(jst_solver* s, double* dt);
+
+/* Solver::residual (solver.rs:190-200) of the last completed step. */
+jst_status jst_residual(jst_solver* s, double* out);
+
+/* Solver public fields `totaltime` and `step` (solver.rs:25-34). */
+jst_status jst_totaltime(const jst_solver* s, double* out);
+jst_status jst_step_count(const jst_solver* s, int64_t* out);
+
+/* Cell fields readable with jst_get_field. */
+typedef enum {
+    JST_F_RHO = 0, JST_F_P, JST_F_T, JST_F_U, JST_F_V, JST_F_E, JST_F_H, JST_F_C, JST_F_NUT,
+    JST_F_U0, JST_F_U1, JST_F_U2, JST_F_U3, JST_F_U4,
+    JST_F_FC0, JST_F_FC1, JST_F_FC2, JST_F_FC3, JST_F_FC4,
+    JST_F_FV0, JST_F_FV1, JST_F_FV2, JST_F_FV3, JST_F_FV4,
+    JST_F_FD0, JST_F_FD1, JST_F_FD2, JST_F_FD3, JST_F_FD4,
+    JST_F_S,
+    JST_F_DUDX, JST_F_DUDY, JST_F_DVDX, JST_F_DVDY, JST_F_DTDX, JST_F_DTDY, JST_F_DNUTDX, JST_F_DNUTDY,
+    JST_F_SA_CHI, JST_F_SA_FV1,
+    JST_F_LOCALDT,
+    JST_F_VOL, JST_F_CX, JST_F_CY, JST_F_WALL_DIST,
+    JST_F_COUNT
+} jst_field;
+
+/* Copies an interior cell field into out[n] (n >= NI*NJ).  Primitive and
+ * conserved fields are available on both paths; the separate residual terms,
+ * gradients and chi/fv1 after jst_residual_terms on the passes path. */
+jst_status jst_get_field(jst_solver* s, int field, double* out, size_t n);
+
+/* Face geometry: which = 0 for tau faces ((NI+1) x NJ), 1 for n faces
+ * (NI x NJ); out receives (nx, ny, mx, my) per face, i-major (geometry.rs:25-34). */
+jst_status jst_get_faces(jst_solver* s, int which, double* out, size_t n);
+
+/* Overwrites the conserved state U (5 planes of NI*NJ, component-major) and
+ * re-derives the primitives (solver.rs:151-185); fails with
+ * JST_ERR_NONPHYSICAL exactly where unpack would. */
+jst_status jst_set_conserved(jst_solver* s, const double* u5, size_t n, jst_nonphysical* bad);
+
+/* Lift and drag coefficients of the current state (no counterpart in the
+ * reference): wall pressure and viscous face fluxes integrated over ring 0,
+ * rotated by the angle of attack and divided by 0.5*rho_inf*V_inf^2*chord,
+ * chord = x-extent of the wall ring.  Runs jst_residual_terms' boundary and
+ * viscous passes on the current state first. */
+jst_status jst_forces(jst_solver* s, double* cl, double* cd);
+
+/* Solver::write_csv (solver.rs:229-255): `i,j,x,y,rho,p,T,u,v,miubl`,
+ * 1-based indices, values in Rust `{:.8e}` format. */
+jst_status jst_write_csv(jst_solver* s, const char* path);
+
+/* Version string of this library. */
+const char* jst_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JST_GPU_H */

@@ -1,0 +1,275 @@
+// Shared device arithmetic for the JST + Spalart-Allmaras stage kernels.
+//
+// Every formula keeps the evaluation order of the reference (jst-rs, cited
+// file:line), so that a translation unit compiled without FMA contraction
+// (the strict FP64 passes path) reproduces the reference's FP64 results, and
+// the fused path differs from it only by contraction/precision.  Functions
+// are templated on the arithmetic type T (double or float); geometry and
+// constants arrive as double and are converted where T = float.
+#pragma once
+
+#include <cstdint>
+#include <cmath>
+
+#ifdef __CUDACC__
+#define JST_HD __host__ __device__ __forceinline__
+#define JST_D __device__ __forceinline__
+#else
+#define JST_HD inline
+#define JST_D inline
+#endif
+
+#ifndef JST_LAUNCH
+#define JST_LAUNCH(kern, grid, block, smem, stream, ...) kern<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__)
+#endif
+
+namespace jst {
+
+// Per-solve constants: config.rs:88-189 inputs and config.rs:191-223 derived
+// values, plus a few constant sub-expressions the reference evaluates inline
+// (each is a pure function of constants, so precomputing it is exact).
+struct PhysConst {
+    double gamma, r_gas, t_suth, cfl, t_inf, p_inf, k2, k4;
+    double Cb1, Cb2, Ct3, Ct4, Cw2, fv3, rmax, sigma;
+    double cv, cp, cw1, cv1_cubed, c_inf, u_inf, v_inf, rho_inf, mu_inf, nut_inf;
+    double suth_num, inv_t_ref, inv_pr, inv_prt, inv_kappa2, cw3_6, one_plus_cw3_6;
+    double gm1;          // gamma - 1.0
+    double rg;           // r_gas * gamma (== gamma * r_gas)
+    double gm1_q;        // (gamma - 1.0) / 4.0          boundary.rs:129
+    double inv_gm1;      // 1.0 / (gamma - 1.0)          boundary.rs:140
+    double half_cfl;     // 0.5 * cfl                    dissipation.rs:61,67
+    double cb1_k2;       // Cb1 * inv_kappa2             source.rs:52
+    double cb2_sigma;    // Cb2 * sigma                  source.rs:53
+    double r_gas_gamma;  // r_gas * gamma                boundary.rs:139 (c^2/(r_gas*gamma))
+    int supersonic;
+    int halo;
+    // Free-stream primitive state written by Cells::initialize (state.rs:522-539).
+    double f_rho, f_p, f_t, f_vx, f_vy, f_e, f_h, f_c, f_nut, f_mu;
+};
+
+// x.powi(n) for the constant exponents the reference uses, expanded by binary
+// decomposition as LLVM lowers powi with a constant exponent.
+template <class T> JST_HD T powi2(T x) { return x * x; }
+template <class T> JST_HD T powi3(T x) { return x * (x * x); }
+template <class T> JST_HD T powi6(T x) {
+    T x2 = x * x;
+    T x4 = x2 * x2;
+    return x2 * x4;
+}
+
+template <class T> JST_HD T tmax(T a, T b) { return fmax(a, b); }
+template <class T> JST_HD T tmin(T a, T b) { return fmin(a, b); }
+template <> JST_HD float tmax<float>(float a, float b) { return fmaxf(a, b); }
+template <> JST_HD float tmin<float>(float a, float b) { return fminf(a, b); }
+
+// Primitive state of one cell.
+template <class T> struct Prim {
+    T rho, p, t, vx, vy, e, nut;
+};
+
+// Solver::unpack (solver.rs:158-181) for one cell, without the checks.
+template <class T> JST_HD Prim<T> unpack_cell(T u0, T u1, T u2, T u3, T u4, T gm1, T r_gas) {
+    Prim<T> q;
+    T rho = u0;
+    T inv = T(1) / rho;
+    q.rho = rho;
+    q.vx = u1 * inv;
+    q.vy = u2 * inv;
+    q.e = u3 * inv;
+    q.p = gm1 * (u3 - rho * (q.vx * q.vx + q.vy * q.vy) * T(0.5));
+    q.t = q.p / (r_gas * rho);
+    q.nut = u4 * inv;
+    return q;
+}
+
+// Cells::pack (state.rs:490-505).
+template <class T> JST_HD void pack_cell(const Prim<T>& q, T* u) {
+    u[0] = q.rho;
+    u[1] = q.rho * q.vx;
+    u[2] = q.rho * q.vy;
+    u[3] = q.rho * q.e;
+    u[4] = q.rho * q.nut;
+}
+
+// Config::mu, Sutherland (config.rs:287-291).
+template <class T> JST_HD T mu_of(T t, T inv_t_ref, T suth_num, T t_suth) {
+    T r = t * inv_t_ref;
+    return r * sqrt(r) * suth_num / (t + t_suth);
+}
+
+// convection::euler_flux (convection.rs:25-40): F.n of the face state fu.
+template <class T> JST_HD void euler_flux(const T fu[5], T nx, T ny, T gm1, T out[5]) {
+    T rho = fu[0];
+    T inv_rho = T(1) / rho;
+    T u = fu[1] * inv_rho;
+    T v = fu[2] * inv_rho;
+    T rho_e = fu[3];
+    T p = gm1 * (rho_e - rho * (u * u + v * v) * T(0.5));
+    T vn = nx * u + ny * v;
+    out[0] = rho * vn;
+    out[1] = fu[1] * vn + p * nx;
+    out[2] = fu[2] * vn + p * ny;
+    out[3] = (rho_e + p) * vn;
+    out[4] = fu[4] * vn;
+}
+
+// Green-Gauss sum of one scalar (gradient.rs:22-35).  c, up, dn, lf, rt are
+// the cell value and its i+1, i-1, j-1, j+1 neighbours; the faces are
+// tau(i+1), tau(i), n(j), n(j+1).
+template <class T>
+JST_HD void green_gauss(T c, T vup, T vdn, T vlf, T vrt, T upx, T upy, T dnx, T dny, T lfx, T lfy, T rtx, T rty,
+                        T inv_v, T* gx, T* gy) {
+    T f_up = T(0.5) * (c + vup);
+    T f_dn = T(0.5) * (c + vdn);
+    T f_lf = T(0.5) * (c + vlf);
+    T f_rt = T(0.5) * (c + vrt);
+    *gx = (f_up * upx - f_dn * dnx + f_rt * rtx - f_lf * lfx) * inv_v;
+    *gy = (f_up * upy - f_dn * dny + f_rt * rty - f_lf * lfy) * inv_v;
+}
+
+// Diffusion tensor columns of one cell (viscous.rs:37-71): returns mu, chi,
+// fv1 and Dx[1..4], Dy[1..4] (component 0 is identically zero).
+template <class T> struct Diff {
+    T mu, chi, fv1;
+    T dx1, dx2, dx3, dx4, dy1, dy2, dy3, dy4;
+};
+
+template <class T>
+JST_HD Diff<T> diffusion_tensor(T t, T rho_nu, T vx, T vy, T dudx, T dudy, T dvdx, T dvdy, T dtdx, T dtdy, T dnx,
+                                T dny, T inv_t_ref, T suth_num, T t_suth, T cv1_cubed, T inv_pr, T inv_prt, T cp,
+                                T sigma) {
+    Diff<T> d;
+    T mu = mu_of<T>(t, inv_t_ref, suth_num, t_suth);
+    T chi = rho_nu / mu;
+    T c3 = chi * chi * chi;  // viscous.rs:27-30
+    T f1 = c3 / (c3 + cv1_cubed);
+    T mu_t = rho_nu * f1;
+    T mu_eff = mu + mu_t;
+    T lam_eff = mu * inv_pr + mu_t * inv_prt;
+    T txx = mu_eff * (T(4.0 / 3.0) * dudx - T(2.0 / 3.0) * dvdy);
+    T tyy = mu_eff * (T(4.0 / 3.0) * dvdy - T(2.0 / 3.0) * dudx);
+    T txy = mu_eff * (dudy + dvdx);
+    T qx = lam_eff * cp * dtdx;
+    T qy = lam_eff * cp * dtdy;
+    T nu_diff = sigma * (mu + rho_nu);
+    d.mu = mu;
+    d.chi = chi;
+    d.fv1 = f1;
+    d.dx1 = txx;
+    d.dx2 = txy;
+    d.dx3 = vx * txx + vy * txy + qx;
+    d.dx4 = nu_diff * dnx;
+    d.dy1 = txy;
+    d.dy2 = tyy;
+    d.dy3 = vx * txy + vy * tyy + qy;
+    d.dy4 = nu_diff * dny;
+    return d;
+}
+
+// dissipation::pressure_sensor (dissipation.rs:29-31).
+template <class T> JST_HD T pressure_sensor(T pm, T p0, T pp) {
+    return fabs((pm - T(2) * p0 + pp) / (pm + T(2) * p0 + pp));
+}
+
+// source::fw (source.rs:30-33).
+template <class T> JST_HD T fw_of(T r, T cw2, T cw3_6, T one_plus_cw3_6) {
+    T g = r + cw2 * (powi6<T>(r) - r);
+    return g * cbrt(sqrt(one_plus_cw3_6 / (powi6<T>(g) + cw3_6)));
+}
+
+// source::compute for one cell (source.rs:55-85), before the factor V.
+template <class T>
+JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny, const PhysConst& c) {
+    T nu_tilde = rho_nu / rho;
+    T inv_kd2 = inv_dist2 * T(c.inv_kappa2);
+    T ft2 = T(c.Ct3) * exp(-T(c.Ct4) * chi * chi);
+    T fv2 = T(1) - chi / (T(1) + chi * f1);
+    T sv = T(c.fv3) * fabs(dvdx - dudy);
+    T s_tilde = tmax<T>(sv + nu_tilde * inv_kd2 * fv2, T(1e-10));
+    T prod = T(c.Cb1) * (T(1) - ft2) * s_tilde * rho_nu;
+    T r = tmin<T>(nu_tilde / s_tilde * inv_kd2, T(c.rmax));
+    T destr = (T(c.cw1) * fw_of<T>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6)) - T(c.cb1_k2) * ft2) * rho *
+              (nu_tilde * nu_tilde * inv_dist2);
+    T diff = T(c.cb2_sigma) * rho * (dnx * dnx + dny * dny);
+    return prod - destr + diff;
+}
+
+// boundary::extrapolate_nut (boundary.rs:158-185).  dist[k], nu[k] belong
+// to cell NI-1-k.
+JST_HD double extrapolate_nut(const double dist[3], const double nu[3]) {
+    const double FLOOR = 1e-10;
+    double l1 = dist[0], l2 = dist[1], l3 = dist[2];
+    double d12 = l1 - l2, d13 = l1 - l3, d23 = l2 - l3;
+    if (fabs(d12) < 1e-14 || fabs(d13) < 1e-14 || fabs(d23) < 1e-14) return fmax(nu[0], FLOOR);
+    double v = l2 * l3 / (d12 * d13) * nu[0] + l1 * l3 / (-d12 * d23) * nu[1] + l1 * l2 / (d23 * -d13) * nu[2];
+    return v > FLOOR ? v : FLOOR;
+}
+
+// boundary::riemann_face (boundary.rs:112-155) for far-field column j, given
+// the tau face NI normal (fnx, fny) and midpoint (fmx, fmy), the primitive
+// state of cell NI-1 (u, v, c) and, for the nu-tilde extrapolation, the
+// centroid distances and nu-tilde of cells NI-1..NI-3.  Returns the face
+// state; h and c of the ghost follow as in far_field_riemann (boundary.rs:93-94).
+struct FarState {
+    double rho, p, t, vx, vy, e, nut;
+    int inflow;
+};
+
+JST_HD FarState riemann_face(double fnx, double fny, double ui, double vi, double ci, const double dist[3],
+                             const double nu[3], const PhysConst& c) {
+    double len = hypot(fnx, fny);
+    double nx = fnx, ny = fny;
+    double gamma = c.gamma;
+    double vn_inf = (c.u_inf * nx + c.v_inf * ny) / len;
+    double vt_inf = (c.u_inf * ny - c.v_inf * nx) / len;
+    double vn_in = (ui * nx + vi * ny) / len;
+    double vt_in = (ui * ny - vi * nx) / len;
+    double c_face, vn_face, vt_face;
+    int inflow;
+    if (!c.supersonic) {
+        double r_in = vn_in + 2.0 * ci / c.gm1;
+        double r_inf = vn_inf - 2.0 * c.c_inf / c.gm1;
+        double vn = 0.5 * (r_in + r_inf);
+        double cf = c.gm1_q * (r_in - r_inf);
+        inflow = vn <= 0.0;
+        c_face = cf;
+        vn_face = vn;
+        vt_face = inflow ? vt_inf : vt_in;
+    } else if (vn_inf <= 0.0) {
+        c_face = c.c_inf;
+        vn_face = vn_inf;
+        vt_face = vt_inf;
+        inflow = 1;
+    } else {
+        c_face = ci;
+        vn_face = vn_in;
+        vt_face = vt_in;
+        inflow = 0;
+    }
+    (void)gamma;
+    FarState s;
+    double t = c_face * c_face / c.r_gas_gamma;
+    double rho = c.rho_inf * pow(t / c.t_inf, c.inv_gm1);
+    double p = rho * c.r_gas * t;
+    double vx = (vt_face * ny + vn_face * nx) / len;
+    double vy = (-vt_face * nx + vn_face * ny) / len;
+    s.rho = rho;
+    s.p = p;
+    s.t = t;
+    s.vx = vx;
+    s.vy = vy;
+    s.e = p / (rho * c.gm1) + 0.5 * (vx * vx + vy * vy);
+    s.nut = inflow ? c.nut_inf : extrapolate_nut(dist, nu);
+    s.inflow = inflow;
+    return s;
+}
+
+// timestep::compute for one cell (timestep.rs:30-42): a,b / cc,dd are the
+// averaged tau / n normals.
+template <class T> JST_HD T local_dt(T u, T v, T cs, T a, T b, T cc, T dd, T cfl_vol) {
+    T conv = fabs(u * a + v * b) + fabs(u * cc + v * dd);
+    T acou = cs * (sqrt(a * a + b * b) + sqrt(cc * cc + dd * dd));
+    return cfl_vol / (conv + acou);
+}
+
+}  // namespace jst
