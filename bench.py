@@ -1,0 +1,317 @@
+#!/usr/bin/env python3
+"""Benchmark of the explicit RANS residual / RK loop on B200.
+
+Workload (default): NACA0012 O-mesh, 4097 x 1025 nodes with a closed ring
+(4096 x 1024 = 4,194,304 cells), far field 30c, wall spacing 1e-6c, M 0.8,
+alpha 1.25 deg, Re 1e7, FP32 fluxes with the FP64 state accumulator, fused
+tiled stage kernels.  A step is one 5-stage RK step over the whole mesh;
+throughput is Mcell-stage/s = cells * 5 * steps / seconds.  The mesh is
+generated here (synthetic, seeded by construction); state + geometry
+(~0.7 GB) exceed the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the CPU restatement of the reference's jst-rs loop
+(oracle/libjst_oracle.so, FP64, OpenMP rows with all host threads) on the
+same workload, a bounded number of steps.  Under torchrun (N > 1) every rank
+solves its own independent instance (replicas, no data-path collective);
+time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "solves/s & p99 at CL/CD err<=1e-4, batched FP32 vs plain FP64; Mcell-stage/s"
+UNIT = "Mcell-stage/s"
+
+# Algorithmic (compulsory) HBM bytes per cell per stage of the fused kernels,
+# averaged over the 5 stages of a step (geometry: tau and n normals 32 B,
+# vol 8, 1/V 8, 1/d^2 8 = 56 B; U_n FP64 40 B; stage state T; ratio T):
+#   FP64:  stage 1: U_n 40 + write 40 + geom 56 + ratio 8                 = 144
+#          stages 2-4: U 40 + U_n 40 + write 40 + geom 56 + ratio 8       = 184
+#          stage 5: U 40 + U_n 40 + write U_n 40 + geom 56 + ratio 8+8    = 192
+#          average 177.6 B
+#   split: stage 1: U_n 40 + write 20 + geom 56 + ratio 4                 = 120
+#          stages 2-4: U 20 + U_n 40 + write 20 + geom 56 + ratio 4       = 140
+#          stage 5: U 20 + U_n 40 + write U_n 40 + geom 56 + ratio 4+4    = 164
+#          average 140.8 B
+BYTES_PER_CELL_STAGE = {"fp64": (144 + 3 * 184 + 192) / 5.0, "split": (120 + 3 * 140 + 164) / 5.0}
+BYTES_PER_STAGE = {"fp64": [144, 184, 184, 184, 192], "split": [120, 140, 140, 140, 164]}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(prec: str):
+    """DRAM bytes per cell-stage of the stage kernel from the committed ncu
+    summary (profiles/stage_kernel_*.md, line `traffic_bytes_per_cell_stage <prec> <value>`)."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for line in f.read_text().splitlines():
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_cell_stage" and parts[1] == prec:
+                try:
+                    return float(parts[2])
+                except ValueError:
+                    pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.zeros(1, device="cuda")
+        dist.all_reduce(t)
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference(workload: str, timed_steps: int, warm_steps: int):
+    """Oracle (CPU restatement of jst-rs, FP64) on the host cores."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import jst_oracle as jo
+    from purinecfd_b200 import workloads
+    cfg, xy, nr, nt = workloads.WORKLOADS[workload]()
+    cores = os.cpu_count() or 1
+    jo.set_threads(cores)
+    t0 = time.perf_counter()
+    o = jo.OracleSolver(cfg, xy, nr, nt)
+    t_setup = time.perf_counter() - t0
+    if warm_steps:
+        o.run(warm_steps)
+    t0 = time.perf_counter()
+    o.run(timed_steps)
+    dt = time.perf_counter() - t0
+    cells = o.n_cells
+    o.close()
+    return {"value": cells * 5 * timed_steps / dt / 1e6, "cores": cores, "seconds": dt, "setup_s": t_setup,
+            "steps": timed_steps, "cells": cells}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 3))
+    warm = 1 if args.warmup > 0 else 0
+    r = cpu_reference(args.workload, steps, warm)
+    sample = (f"{args.workload}: {r['cells']} cells, {warm} untimed + {steps} timed RK steps of the oracle "
+              f"(CPU FP64 restatement of jst-rs; Rust toolchain absent), {r['cores']} OpenMP threads")
+    line = {"metric": METRIC, "value": round(r["value"], 3), "unit": UNIT, "n_gpus": 0, "steps": steps,
+            "warmup": warm, "ms_per_step": round(1e3 * r["seconds"] / steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.workload, "precision": "fp64", "path": "cpu oracle"},
+            "cpu_baseline": {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(r["value"], 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    from purinecfd_b200 import PATH_FUSED, PREC_FP32_SPLIT, PREC_FP64, Solver, workloads
+    prec = PREC_FP32_SPLIT if args.precision == "split" else PREC_FP64
+    cfg, xy, nr, nt = workloads.WORKLOADS[args.workload]()
+    s = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=local)
+    cells = s.n_cells
+    s.time_steps(args.warmup)
+    barrier(world)
+    with ClockSampler(local) as clk:
+        ms, _ = s.time_steps(args.steps)
+    barrier(world)
+    ms_max = max_over_ranks(ms, world)
+    _, stage_ms = s.time_steps(0, stages=True)
+    residual = s.residual()
+    s.close()
+    value = world * cells * 5 * args.steps / (ms_max / 1e3) / 1e6
+
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "split" else "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "cells": cells, "precision": args.precision,
+                       "path": "fused tiled stage kernel, CUDA graph per RK step",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (state + geometry ~0.7 GB)"},
+            "gpu_launches": 5 * args.steps, "residual_after": residual}
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        bps = BYTES_PER_CELL_STAGE[args.precision]
+        stage_avg = sum(stage_ms) / 5.0
+        achieved = bps * cells / (stage_avg / 1e3) / 1e9
+        trafc = ncu_traffic(args.precision)
+        line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                            "traffic": None if trafc is None else round(trafc * cells),
+                            "kernel": "k_stage (5 launches per step; stage times " +
+                                      ", ".join(f"{x:.3f}" for x in stage_ms) + " ms)",
+                            "bytes_per_cell_stage": round(bps, 1)}
+        line["clocks"] = clk.summary()
+        if world == 1 and not args.no_fp64:
+            s64 = Solver(cfg, xy, nr, nt, precision=PREC_FP64, kernel_path=PATH_FUSED, device=local)
+            s64.time_steps(3)
+            k64 = max(5, min(args.steps, 100))
+            ms64, st64 = s64.time_steps(k64, stages=True)
+            v64 = cells * 5 * k64 / (ms64 / 1e3) / 1e6
+            a64 = BYTES_PER_CELL_STAGE["fp64"] * cells / (sum(st64) / 5.0 / 1e3) / 1e9
+            line["fp64_plain"] = {"value": round(v64, 3), "unit": UNIT, "steps": k64,
+                                  "ms_per_step": round(ms64 / k64, 5),
+                                  "roofline": {"achieved": round(a64, 1), "peak": peak, "unit": "GB/s",
+                                               "frac": round(a64 / peak, 4),
+                                               "bytes_per_cell_stage": BYTES_PER_CELL_STAGE["fp64"]}}
+            s64.close()
+        # end to end through the public API from host buffers: create (mesh H2D,
+        # geometry on the GPU), K steps with the per-step residual read back,
+        # final fields D2H
+        if not args.no_e2e:
+            fields = ("rho", "u", "v", "p", "T", "nut")
+            t0 = time.perf_counter()
+            se = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=local)
+            hist = []
+            se.run(args.steps, lambda k, r: hist.append(r))
+            out = [se.get(f) for f in fields]
+            t_e2e = time.perf_counter() - t0
+            se.close()
+            h2d = xy.size * 8 + len(json.dumps(cfg))
+            d2h = sum(a.nbytes for a in out) + 8 * args.steps
+            line["e2e"] = {"value": round(cells * 5 * args.steps / t_e2e / 1e6, 3), "unit": UNIT,
+                           "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+                           "seconds": round(t_e2e, 4),
+                           "what": "jst_create from host nodes + jst_run with per-step residual callback + "
+                                   "6 fields read back"}
+        if world == 1 and not args.no_cpu:
+            r = cpu_reference(args.workload, 2, 1)
+            line["cpu_baseline"] = {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
+                                    "sample": f"{args.workload}: {r['cells']} cells, 1 untimed + 2 timed RK steps, "
+                                              f"oracle (CPU FP64 restatement of jst-rs), {r['cores']} threads"}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="naca0012_4097x1025")
+    ap.add_argument("--precision", choices=["split", "fp64"], default="split")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain-path line")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                   int(os.environ.get("RANK", "0")), 0)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -186,6 +186,13 @@ jst_status jst_forces(jst_solver* s, double* cl, double* cd);
  * 1-based indices, values in Rust `{:.8e}` format. */
 jst_status jst_write_csv(jst_solver* s, const char* path);
 
+/* Device timing (no counterpart in the reference; used by benchmarks):
+ * enqueues nsteps RK steps with the convergence test disabled and returns
+ * their device time in *ms, measured with CUDA events on the solver's own
+ * stream.  When stage_ms is non-NULL one further step is run stage by stage
+ * and stage_ms[0..4] receive the five stage kernels' times. */
+jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_ms);
+
 /* Version string of this library. */
 const char* jst_version(void);
 

@@ -492,6 +492,7 @@ double timestep_compute(Solver& s) {
             s.localdt(i, j) = cfl * s.vol(i, j) / (conv + acou);
         }
     double m = std::numeric_limits<double>::infinity();
+#pragma omp parallel for schedule(static) reduction(min : m)
     for (long i = 0; i < s.ni; ++i)
         for (long j = 0; j < nj; ++j) m = std::fmin(m, s.localdt(i, j));
     return m;
@@ -677,10 +678,12 @@ void dissipation_compute(Solver& s) {
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < ni; ++i)
         for (long j = 0; j < nj; ++j) s.spec_ratio(i, j) = s.vol(i, j) / s.localdt(i, j);
+#pragma omp parallel for schedule(static)
     for (long i = 0; i <= ni; ++i) {
         long a = std::min(std::max(i, 0L), ni - 1), b = std::min(std::max(i - 1, 0L), ni - 1);
         for (long j = 0; j < nj; ++j) s.tlam[(size_t)i * nj + j] = 0.5 * cfl * (s.spec_ratio(a, j) + s.spec_ratio(b, j));
     }
+#pragma omp parallel for schedule(static)
     for (long i = 0; i < ni; ++i)
         for (long j = 0; j < nj; ++j) {
             long jm = j > 0 ? j - 1 : nj - 1;
@@ -692,6 +695,7 @@ void dissipation_compute(Solver& s) {
     for (long i = 0; i < ni; ++i)
         for (long j = -2; j <= nj; ++j) s.sensor_j(i, j) = pressure_sensor(s.p(i, j - 1), s.p(i, j), s.p(i, j + 1));
     // coefficients 93-126 (adaptive_coefficients 35-38)
+#pragma omp parallel for schedule(static)
     for (long i = 0; i <= ni; ++i)
         for (long j = 0; j < nj; ++j) {
             double m = std::fmax(std::fmax(std::fmax(s.sensor_i(i - 2, j), s.sensor_i(i - 1, j)), s.sensor_i(i, j)),
@@ -700,6 +704,7 @@ void dissipation_compute(Solver& s) {
             s.te2[(size_t)i * nj + j] = e2;
             s.te4[(size_t)i * nj + j] = std::fmax(k4 - e2, 0.0);
         }
+#pragma omp parallel for schedule(static)
     for (long i = 0; i < ni; ++i)
         for (long j = 0; j < nj; ++j) {
             double m = std::fmax(std::fmax(std::fmax(s.sensor_j(i, j - 2), s.sensor_j(i, j - 1)), s.sensor_j(i, j)),

@@ -236,6 +236,7 @@ class PassesEngine : public Engine {
         passes_set_uniform(P_, core_->c, rho, vx, vy, p, nut, core_->st);
     }
     void run_kernel(const char* name) override { passes_kernel(P_, core_->g, core_->c, name, core_->st); }
+    cudaStream_t stream() const override { return core_->st; }
 
   private:
     SolverCore* core_;
@@ -600,6 +601,18 @@ jst_status jst_write_csv(jst_solver* s, const char* path) {
         }
     std::fclose(f);
     return JST_OK;
+}
+
+jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_ms) {
+    if (!s || !ms || nsteps < 0) return JST_ERR_ARG;
+    int64_t before = 0;
+    jst_status rc = s->eng->time_steps(nsteps, ms, stage_ms);
+    (void)before;
+    if (rc == JST_OK) {
+        s->step += nsteps + (stage_ms ? 1 : 0);
+        s->eng->residual(&s->last_residual);
+    }
+    return rc;
 }
 
 // Test hooks (not in the public header): uniform state on every cell and a

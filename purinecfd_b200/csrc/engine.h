@@ -46,6 +46,25 @@ class Engine {
     virtual jst_status wall_force(double* fx, double* fy) = 0;
     virtual jst_status residual(double* out) = 0;
     virtual jst_status totaltime(double* out) = 0;
+    virtual jst_status time_steps(int nsteps, double* ms, double* stage_ms) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, stream());
+        jst_status rc = JST_OK;
+        for (int k = 0; k < nsteps && rc == JST_OK; ++k) rc = advance(nullptr);
+        cudaEventRecord(b, stream());
+        cudaEventSynchronize(b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        *ms = t;
+        if (stage_ms)
+            for (int k = 0; k < 5; ++k) stage_ms[k] = -1.0;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return rc;
+    }
+    virtual cudaStream_t stream() const = 0;
     virtual void set_uniform(double, double, double, double, double) {}
     virtual void run_kernel(const char*) {}
 

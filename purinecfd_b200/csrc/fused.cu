@@ -316,15 +316,19 @@ template <class T> class FusedEngine : public Engine {
             enqueue_step(st);
             return;
         }
-        if (!graph_exec_) {
-            cudaGraph_t g;
-            cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-            enqueue_step(st);
-            cudaStreamEndCapture(st, &g);
-            cudaGraphInstantiate(&graph_exec_, g, 0);
-            cudaGraphDestroy(g);
-        }
+        ensure_graph();
         cudaGraphLaunch(graph_exec_, st);
+    }
+
+    void ensure_graph() {
+        if (graph_exec_ || !core_->opts.use_graph) return;
+        cudaStream_t st = core_->st;
+        cudaGraph_t g;
+        cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        enqueue_step(st);
+        cudaStreamEndCapture(st, &g);
+        cudaGraphInstantiate(&graph_exec_, g, 0);
+        cudaGraphDestroy(g);
     }
 
     jst_status read_state(InstState* out) {
@@ -536,11 +540,51 @@ template <class T> class FusedEngine : public Engine {
         return JST_OK;
     }
 
-    // Bench hooks: enqueue k steps without synchronising, and the tile count.
-    void enqueue_steps(int k) {
-        for (int q = 0; q < k; ++q) launch_step();
+    cudaStream_t stream() const override { return core_->st; }
+
+    // nsteps graph-replayed steps with the target disabled, timed with CUDA
+    // events on the solver stream; optionally one more step stage by stage.
+    jst_status time_steps(int nsteps, double* ms, double* stage_ms) override {
+        cudaStream_t st = core_->st;
+        InstState s;
+        if (read_state(&s) != JST_OK) return JST_ERR_CUDA;
+        double never = -1.0;
+        int zero = 0;
+        cudaMemcpyAsync(&inst_.st->target, &never, sizeof never, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(&inst_.st->done, &zero, sizeof zero, cudaMemcpyHostToDevice, st);
+        int total = nsteps + (stage_ms ? 1 : 0);
+        if ((size_t)(s.step + total) > hist_cap_) grow_hist((size_t)(s.step + total));
+        set_max_step(s.step + total);
+        ensure_graph();
+        cudaEvent_t ev[8];  // 0,1: around the steps; 2..7: stage boundaries of the extra step
+        for (auto& e : ev) cudaEventCreate(&e);
+        cudaEventRecord(ev[0], st);
+        for (int q = 0; q < nsteps; ++q) launch_step();
+        cudaEventRecord(ev[1], st);
+        if (stage_ms) {
+            cudaEventRecord(ev[2], st);
+            for (int q = 0; q < 5; ++q) {
+                auto kern = q == 0 ? K_.stage[0] : (q == 4 ? K_.stage[2] : K_.stage[1]);
+                JST_LAUNCH(kern, ntiles_, K_.nt, K_.smem, st, d_tiles_, d_inst_, q, RK_ALPHA[q]);
+                cudaEventRecord(ev[3 + q], st);
+            }
+        }
+        if (cudaEventSynchronize(stage_ms ? ev[7] : ev[1]) != cudaSuccess) return JST_ERR_CUDA;
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[0], ev[1]);
+        *ms = t;
+        if (stage_ms)
+            for (int q = 0; q < 5; ++q) {
+                float tq = 0.f;
+                cudaEventElapsedTime(&tq, ev[2 + q], ev[3 + q]);
+                stage_ms[q] = tq;
+            }
+        for (auto& e : ev) cudaEventDestroy(e);
+        cudaMemcpyAsync(&inst_.st->target, &core_->targetres, sizeof(double), cudaMemcpyHostToDevice, st);
+        if (read_state(&s) != JST_OK) return JST_ERR_CUDA;
+        if (s.bad != fused::NO_BAD) return JST_ERR_NONPHYSICAL;
+        return JST_OK;
     }
-    int ntiles() const { return ntiles_; }
 
   private:
     SolverCore* core_;

@@ -63,15 +63,21 @@ def ellipse_o_mesh(n_rings: int, n_theta: int, a_wall: float = 1.0, b_wall: floa
 
 
 def geometric_ratio(first: float, total: float, n_intervals: int) -> float:
-    """Ratio q with first*(q**n - 1)/(q - 1) == total (bisection, q >= 1)."""
+    """Ratio q with first*(q**n - 1)/(q - 1) == total (bisection in log space, q >= 1)."""
     if first * n_intervals >= total:
         return 1.0
-    lo, hi = 1.0 + 1e-15, 2.0
-    while first * (hi ** n_intervals - 1.0) / (hi - 1.0) < total:
+
+    def log_sum(q):  # log(first * (q**n - 1) / (q - 1)) without overflow
+        a = n_intervals * math.log(q)
+        return math.log(first) + a + math.log(-math.expm1(-a)) - math.log(q - 1.0)
+
+    target = math.log(total)
+    lo, hi = 1.0 + 1e-12, 2.0
+    while log_sum(hi) < target:
         hi *= 2.0
     for _ in range(200):
         mid = 0.5 * (lo + hi)
-        if first * (mid ** n_intervals - 1.0) / (mid - 1.0) < total:
+        if log_sum(mid) < target:
             lo = mid
         else:
             hi = mid

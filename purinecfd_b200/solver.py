@@ -42,7 +42,7 @@ FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
 EXPORTS = ["jst_default_opts", "jst_create_from_paths", "jst_create", "jst_destroy", "jst_last_error", "jst_ni",
            "jst_nj", "jst_advance", "jst_run", "jst_residual_terms", "jst_timestep", "jst_residual",
            "jst_totaltime", "jst_step_count", "jst_get_field", "jst_get_faces", "jst_set_conserved",
-           "jst_forces", "jst_write_csv", "jst_version"]
+           "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps"]
 
 
 class Opts(C.Structure):
@@ -117,6 +117,7 @@ def lib() -> C.CDLL:
         L.jst_forces.argtypes = [vp, pd, pd]
         L.jst_write_csv.argtypes = [vp, C.c_char_p]
         L.jst_version.restype = C.c_char_p
+        L.jst_time_steps.argtypes = [vp, i, pd, pd]
         L.jst_debug_set_uniform.argtypes = [vp, d, d, d, d, d]
         L.jst_debug_kernel.argtypes = [vp, C.c_char_p]
         _lib = L
@@ -267,6 +268,15 @@ class Solver:
     def write_csv(self, path):
         """Solver::write_csv (solver.rs:229-255)."""
         self._check(lib().jst_write_csv(self._h, str(path).encode()))
+
+    def time_steps(self, nsteps: int, stages: bool = False):
+        """Device time (ms) of `nsteps` RK steps with the convergence test off,
+        measured with CUDA events on the solver's stream; with stages=True one
+        more step runs stage by stage and its five stage times are returned."""
+        ms = C.c_double(0.0)
+        st = np.zeros(5)
+        self._check(lib().jst_time_steps(self._h, int(nsteps), C.byref(ms), _ptr(st) if stages else None))
+        return ms.value, (st.tolist() if stages else None)
 
     # test hooks
     def set_uniform(self, rho, vx, vy, p, nut):
