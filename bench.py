@@ -210,7 +210,11 @@ def run_ours(args, world, rank, local):
     from purinecfd_b200 import PATH_FUSED, PREC_FP32_SPLIT, PREC_FP64, Solver, workloads
     prec = PREC_FP32_SPLIT if args.precision == "split" else PREC_FP64
     cfg, xy, nr, nt = workloads.WORKLOADS[args.workload]()
-    s = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=local)
+    tile = {}
+    if args.tile:
+        ti, tj = (int(x) for x in args.tile.lower().split("x"))
+        tile = {"tile_i": ti, "tile_j": tj}
+    s = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=local, **tile)
     cells = s.n_cells
     s.time_steps(args.warmup)
     barrier(world)
@@ -229,6 +233,7 @@ def run_ours(args, world, rank, local):
             "dtype": "f32+f64" if args.precision == "split" else "f64", "data": "synthetic",
             "config": {"workload": args.workload, "cells": cells, "precision": args.precision,
                        "path": "fused tiled stage kernel, CUDA graph per RK step",
+                       "tile": args.tile or "default",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (state + geometry ~0.7 GB)"},
             "gpu_launches": 5 * args.steps, "residual_after": residual}
@@ -294,6 +299,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="naca0012_4097x1025")
     ap.add_argument("--precision", choices=["split", "fp64"], default="split")
+    ap.add_argument("--tile", default="", help="fused tile TIxTJ (default: the library's choice)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain-path line")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")

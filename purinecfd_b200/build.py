@@ -31,7 +31,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-
 # source -> extra flags
 UNITS = {
     "passes.cu": ["--fmad=false"],
-    "fused.cu": [],
+    "fused.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "api.cu": [],
 }
 

@@ -129,7 +129,7 @@ __global__ void k_wall_force(Geom g, const double* const* un, PhysConst c, int f
 template <class T> size_t stage_smem(int ti, int tj);
 
 // Tile configurations compiled into the library: (TI, TJ, NT).
-#define JST_FOR_TILES(X) X(8, 32, 256) X(16, 32, 256) X(8, 64, 256) X(4, 64, 256)
+#define JST_FOR_TILES(X) X(4, 32, 256) X(8, 32, 256) X(16, 32, 256) X(4, 64, 256) X(8, 64, 256)
 
 template <class T> struct Kernels {
     void (*stage[3])(const TileRef*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};  // first, mid, last

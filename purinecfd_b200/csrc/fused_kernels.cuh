@@ -20,7 +20,12 @@
 // work items separated by barriers.
 #pragma once
 
+#include <cstring>
 #include <type_traits>
+
+#ifdef __CUDACC__
+#include <cuda_pipeline.h>
+#endif
 
 #include "jst_common.cuh"
 
@@ -78,23 +83,33 @@ struct TileRef {
     int inst, i0, j0, tile;  // tile = index within its instance
 };
 
+// Shared-memory layout of one tile.  T-typed arrays first, then the FP64
+// block (geometry and the tile's U_n), then the reduction / far-field
+// scratch.  The primitive arrays (P, Q) are dead once gradients and sensors
+// exist, and the face fluxes reuse their space.
 template <class T, int TI, int TJ, int NT> struct Layout {
     static constexpr int LI = TI + 6, LJ = TJ + 6, NL = LI * LJ;  // staged cells (halo 3)
     static constexpr int RI = TI + 2, RJ = TJ + 2, NR = RI * RJ;  // tile + first ring
+    static constexpr int TT = TI * TJ;
     static constexpr int NSI = (TI + 4) * TJ, NSJ = TI * (TJ + 4);
-    static constexpr int NFT = (TI + 1) * TJ, NFN = TI * (TJ + 1);
-    // offsets in elements of T
+    static constexpr int GTJ = TJ + 2, NGT = (TI + 3) * GTJ;  // tau normals, rows i0-1..i0+TI+1
+    static constexpr int GNJ = TJ + 3, NGN = (TI + 2) * GNJ;  // n normals, rows i0-1..i0+TI
+    // T-typed offsets
     static constexpr int oU = 0;
-    static constexpr int oP = oU + 5 * NL;
-    static constexpr int oQ = oP + NL;  // u, v, T, nut
-    static constexpr int oSi = oQ + 4 * NL;
+    static constexpr int oSi = oU + 5 * NL;
     static constexpr int oSj = oSi + NSI;
-    static constexpr int oD = oSj + NSJ;  // Dx1..4, Dy1..4
-    static constexpr int oG = oD + 8 * NR;  // dvdx, dudy, dnutdx, dnutdy, chi, fv1 (tile cells)
-    static constexpr int oFt = oG + 6 * TI * TJ;
-    static constexpr int oFn = oFt + 5 * NFT;
-    static constexpr int total = oFn + 5 * NFN;
-    static constexpr size_t red_off = ((size_t)total * sizeof(T) + 15) / 16 * 16;  // reduction + far buffers
+    static constexpr int oD = oSj + NSJ;  // Dx1..4, Dy1..4 on tile + ring
+    static constexpr int oS = oD + 8 * NR;  // SA source * V, tile cells
+    static constexpr int oR = oS + TT;      // ratio V/localdt on tile + ring (rows clamped)
+    static constexpr int NFT = (TI + 1) * TJ, NFN = TI * (TJ + 1);
+    static constexpr int oX = oR + NR;      // P (NL) + Q (4 NL)  |  face fluxes Ft (5 NFT) + Fn (5 NFN)
+    static constexpr int XSZ = 5 * NL > 5 * (NFT + NFN) ? 5 * NL : 5 * (NFT + NFN);
+    static constexpr int tsize = oX + XSZ;
+    // FP64 geometry block: tau nx, ny; n nx, ny; 1/V on tile + ring; V and 1/d^2 on the tile
+    static constexpr size_t goff = ((size_t)tsize * sizeof(T) + 15) / 16 * 16;
+    static constexpr int gTx = 0, gTy = NGT, gNx = 2 * NGT, gNy = 2 * NGT + NGN, gIV = 2 * NGT + 2 * NGN,
+                         gV = gIV + NR, gD2 = gV + TT, gUn = gD2 + TT, gsize = gUn + 5 * TT;
+    static constexpr size_t red_off = goff + (size_t)gsize * sizeof(double);
     static constexpr size_t bytes = red_off + (size_t)(NT + 7 * LJ) * sizeof(double);
 };
 
@@ -253,6 +268,22 @@ __global__ void __launch_bounds__(NT) k_step_dt(const TileRef* tiles, const Inst
     }
 }
 
+// Asynchronous global -> shared copies (cp.async), one element each.
+template <int BYTES> JST_D void async_copy(void* dst, const void* src) {
+#ifdef __CUDA_ARCH__
+    __pipeline_memcpy_async(dst, src, BYTES);
+#else
+    std::memcpy(dst, src, BYTES);
+#endif
+}
+
+JST_D void async_wait_all() {
+#ifdef __CUDA_ARCH__
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
+#endif
+}
+
 // The stage kernel.  FIRST: stage 0 (reads U_n, adds dt to the total time).
 // LAST: stage 4 (writes U_n in place, residual, next step's time step).
 template <class T, int TI, int TJ, int NT, bool FIRST, bool LAST>
@@ -260,10 +291,13 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
     using L = Layout<T, TI, TJ, NT>;
     using TS = typename std::conditional<FIRST, double, T>::type;
     using TD = typename std::conditional<LAST, double, T>::type;
+    constexpr bool ASYNC_U = std::is_same<TS, T>::value;
+    constexpr int LJ = L::LJ, NL = L::NL, RJ = L::RJ, NR = L::NR, TT = L::TT;
     JST_DYN_SMEM(smem_raw);
     T* sm = reinterpret_cast<T*>(smem_raw);
+    double* gs = reinterpret_cast<double*>(smem_raw + L::goff);
     double* red = reinterpret_cast<double*>(smem_raw + L::red_off);
-    double* farbuf = red + NT;  // 7 values per staged column when the tile touches the far field
+    double* farbuf = red + NT;  // 7 values per staged column of a far-field tile
     __shared__ int flags[4];
 
     const TileRef tr = tiles[JST_BID()];
@@ -287,6 +321,9 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
     if (flags[0]) return;
     const int fresh = flags[1];
     const unsigned long long stage_id = (unsigned long long)flags[2] * 5 + stage;
+    const T* ratio = I.ratio[flags[2] & 1];
+    T* ratio_next = I.ratio[(flags[2] + 1) & 1];
+    (void)ratio_next;
 
     const TS* src[5];
     TD* dst[5];
@@ -297,41 +334,139 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
         else dst[k] = reinterpret_cast<TD*>((stage % 2 == 0) ? I.ua[k] : I.ub[k]);
     }
 
-    const T* ratio = I.ratio[flags[2] & 1];
-    T* ratio_next = I.ratio[(flags[2] + 1) & 1];
-    (void)ratio_next;
     T* sU = sm + L::oU;
-    T* sP = sm + L::oP;
-    T* sQ = sm + L::oQ;
     T* sSi = sm + L::oSi;
     T* sSj = sm + L::oSj;
     T* sD = sm + L::oD;
-    T* sG = sm + L::oG;
-    T* sFt = sm + L::oFt;
-    T* sFn = sm + L::oFn;
-    constexpr int LJ = L::LJ, NL = L::NL, RJ = L::RJ, NR = L::NR;
+    T* sS = sm + L::oS;
+    T* sRat = sm + L::oR;
+    T* sP = sm + L::oX;
+    T* sQ = sP + NL;        // u, v, T, nut
 
-    // ---- far-field states of the staged columns (boundary.rs:87-155) -----
-    const bool touches_far = i0 + TI + 3 > ni;
-    if (touches_far) {
+    // ---- A1: stage the tile geometry and the interior rows of U ----------
+    for (int e = tid; e < L::NGT; e += NT) {  // tau normals, rows i0-1 .. i0+TI+1
+        int r = e / L::GTJ, cc = e - r * L::GTJ;
+        int gi = i0 - 1 + r, gj = wrapj(j0 - 1 + cc, nj);
+        if (gi >= 0 && gi <= ni) {
+            long f = (long)gi * nj + gj;
+            async_copy<8>(gs + L::gTx + e, I.tnx + f);
+            async_copy<8>(gs + L::gTy + e, I.tny + f);
+        } else {
+            gs[L::gTx + e] = 0.0;
+            gs[L::gTy + e] = 0.0;
+        }
+    }
+    for (int e = tid; e < L::NGN; e += NT) {  // n normals, rows i0-1 .. i0+TI
+        int r = e / L::GNJ, cc = e - r * L::GNJ;
+        int gi = i0 - 1 + r, gj = wrapj(j0 - 1 + cc, nj);
+        if (gi >= 0 && gi < ni) {
+            long f = (long)gi * nj + gj;
+            async_copy<8>(gs + L::gNx + e, I.nnx + f);
+            async_copy<8>(gs + L::gNy + e, I.nny + f);
+        } else {
+            gs[L::gNx + e] = 0.0;
+            gs[L::gNy + e] = 0.0;
+        }
+    }
+    for (int e = tid; e < NR; e += NT) {  // 1/V and V/localdt on tile + ring
+        int r = e / RJ, cc = e - r * RJ;
+        int gi = i0 - 1 + r, gj = wrapj(j0 - 1 + cc, nj);
+        if (gi >= 0 && gi < ni) async_copy<8>(gs + L::gIV + e, I.inv_vol + (long)gi * nj + gj);
+        else gs[L::gIV + e] = 0.0;
+        int gc = gi < 0 ? 0 : (gi > ni - 1 ? ni - 1 : gi);  // dissipation.rs:59 clamps
+        async_copy<sizeof(T)>(sRat + e, ratio + (long)gc * nj + gj);
+    }
+    for (int e = tid; e < TT; e += NT) {  // V and 1/d^2 on the tile
+        int r = e / TJ, cc = e - r * TJ;
+        int gi = i0 + r, gj = wrapj(j0 + cc, nj);
+        if (gi < ni) {
+            async_copy<8>(gs + L::gV + e, I.vol + (long)gi * nj + gj);
+            async_copy<8>(gs + L::gD2 + e, I.inv_d2 + (long)gi * nj + gj);
+        } else {
+            gs[L::gV + e] = 0.0;
+            gs[L::gD2 + e] = 0.0;
+        }
+    }
+    for (int e = tid; e < TT; e += NT) {  // U_n of the tile cells, for the update
+        int r = e / TJ, cc = e - r * TJ;
+        int gi = i0 + r, gj = j0 + cc;
+        if (gi < ni && gj < nj)
+            for (int k = 0; k < 5; ++k) async_copy<8>(gs + L::gUn + k * TT + e, I.un[k] + (long)gi * nj + gj);
+    }
+    constexpr int KA = (NL + NT - 1) / NT;
+    TS rawr[ASYNC_U ? 1 : KA][5];
+#pragma unroll
+    for (int q = 0; q < KA; ++q) {
+        int w = tid + q * NT;
+        if (w < NL) {
+            int li = w / LJ, lj = w - li * LJ;
+            int gi = i0 - 3 + li;
+            if (gi >= 0 && gi < ni) {
+                long id = (long)gi * nj + wrapj(j0 - 3 + lj, nj);
+                if constexpr (ASYNC_U) {
+                    for (int k = 0; k < 5; ++k) async_copy<sizeof(T)>(sU + k * NL + w, src[k] + id);
+                } else {
+                    for (int k = 0; k < 5; ++k) rawr[q][k] = ld(src[k] + id);
+                }
+            }
+        }
+    }
+    async_wait_all();
+    // primitives of the interior rows; periodic ghost columns are re-packed
+    // from their primitives (boundary.rs:54-72, state.rs:490-505)
+#pragma unroll
+    for (int q = 0; q < KA; ++q) {
+        int w = tid + q * NT;
+        if (w < NL) {
+            int li = w / LJ, lj = w - li * LJ;
+            int gi = i0 - 3 + li, gjr = j0 - 3 + lj;
+            if (gi >= 0 && gi < ni) {
+                T u[5];
+                if constexpr (ASYNC_U) {
+                    for (int k = 0; k < 5; ++k) u[k] = sU[k * NL + w];
+                } else {
+                    for (int k = 0; k < 5; ++k) u[k] = (T)rawr[q][k];
+                }
+                Prim<T> p;
+                if (fresh) {
+                    p.rho = (T)c.f_rho;
+                    p.p = (T)c.f_p;
+                    p.t = (T)c.f_t;
+                    p.vx = (T)c.f_vx;
+                    p.vy = (T)c.f_vy;
+                    p.e = (T)c.f_e;
+                    p.nut = (T)c.f_nut;
+                } else {
+                    p = unpack_cell<T>(u[0], u[1], u[2], u[3], u[4], (T)c.gm1, (T)c.r_gas);
+                }
+                bool seam = gjr < 0 || gjr >= nj;
+                if (seam) pack_cell<T>(p, u);
+                if (seam || !ASYNC_U)
+                    for (int k = 0; k < 5; ++k) sU[k * NL + w] = u[k];
+                sP[w] = p.p;
+                sQ[0 * NL + w] = p.vx;
+                sQ[1 * NL + w] = p.vy;
+                sQ[2 * NL + w] = p.t;
+                sQ[3 * NL + w] = p.nut;
+            }
+        }
+    }
+    JST_SYNC();
+
+    // ---- A2: ghost rows from the staged primitives -----------------------
+    const bool wall_tile = i0 == 0;
+    const bool far_tile = i0 + TI + 3 > ni;
+    if (far_tile) {  // far-field state per staged column (boundary.rs:87-155)
+        const int lrow = ni - 1 - i0 + 3;  // staged row of cell NI-1
         for (int lj = tid; lj < LJ; lj += NT) {
             int gj = wrapj(j0 - 3 + lj, nj);
-            long cid = (long)(ni - 1) * nj + gj;
-            T u[5];
-            Prim<T> q = prim_from<T, TS>(src, cid, fresh, c, u);
-            double nu[3], dist[3];
-            nu[0] = (double)q.nut;
-            for (int k = 1; k < 3; ++k) {
-                T u2[5];
-                Prim<T> q2 = prim_from<T, TS>(src, (long)(ni - 1 - k) * nj + gj, fresh, c, u2);
-                nu[k] = (double)q2.nut;
-            }
+            int o = lrow * LJ + lj;
+            double nu[3] = {(double)sQ[3 * NL + o], (double)sQ[3 * NL + o - LJ], (double)sQ[3 * NL + o - 2 * LJ]};
             const double* fg = I.far + 5 * (long)gj;
-            dist[0] = ld(fg + 2);
-            dist[1] = ld(fg + 3);
-            dist[2] = ld(fg + 4);
-            double cs = fresh ? c.f_c : sqrt(c.rg * (double)q.t);
-            FarState f = riemann_face(ld(fg + 0), ld(fg + 1), (double)q.vx, (double)q.vy, cs, dist, nu, c);
+            double dist[3] = {ld(fg + 2), ld(fg + 3), ld(fg + 4)};
+            double t = (double)sQ[2 * NL + o];
+            double cs = fresh ? c.f_c : sqrt(c.rg * t);
+            FarState f = riemann_face(ld(fg + 0), ld(fg + 1), (double)sQ[o], (double)sQ[NL + o], cs, dist, nu, c);
             double* fb = farbuf + 7 * lj;
             fb[0] = f.rho;
             fb[1] = f.p;
@@ -343,74 +478,75 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
         }
         JST_SYNC();
     }
-
-    // ---- phase A: stage the tile + halo, build ghosts, primitives ---------
-    for (int w = tid; w < NL; w += NT) {
-        int li = w / LJ, lj = w - li * LJ;
-        int gi = i0 - 3 + li, gjr = j0 - 3 + lj;
-        int gj = wrapj(gjr, nj);
-        T u[5];
-        Prim<T> q;
-        if (gi >= 0 && gi < ni) {
-            q = prim_from<T, TS>(src, (long)gi * nj + gj, fresh, c, u);
-            if (gjr < 0 || gjr >= nj) pack_cell<T>(q, u);  // periodic ghost (boundary.rs:54-72)
-        } else if (gi < 0) {
-            int k = -1 - gi;  // wall mirror of cell k (boundary.rs:30-51)
-            q = prim_from<T, TS>(src, (long)k * nj + gj, fresh, c, u);
-            q.vx = -q.vx;
-            q.vy = -q.vy;
-            q.nut = -q.nut;
+    if (wall_tile || far_tile) {
+        for (int w = tid; w < NL; w += NT) {
+            int li = w / LJ, lj = w - li * LJ;
+            int gi = i0 - 3 + li;
+            if (gi >= 0 && gi < ni) continue;
+            Prim<T> q;
+            if (gi < 0) {  // wall mirror of cell k = -1-gi (boundary.rs:30-51)
+                int os = (-1 - gi + 3) * LJ + lj;
+                q.rho = sU[os];
+                q.p = sP[os];
+                q.t = sQ[2 * NL + os];
+                q.vx = -sQ[os];
+                q.vy = -sQ[NL + os];
+                q.nut = -sQ[3 * NL + os];
+                q.e = fresh ? (T)c.f_e : sU[3 * NL + os] * (T(1) / q.rho);
+            } else {
+                const double* fb = farbuf + 7 * lj;
+                q.rho = (T)fb[0];
+                q.p = (T)fb[1];
+                q.t = (T)fb[2];
+                q.vx = (T)fb[3];
+                q.vy = (T)fb[4];
+                q.e = (T)fb[5];
+                q.nut = (T)fb[6];
+            }
+            T u[5];
             pack_cell<T>(q, u);
-        } else {
-            const double* fb = farbuf + 7 * lj;
-            q.rho = (T)fb[0];
-            q.p = (T)fb[1];
-            q.t = (T)fb[2];
-            q.vx = (T)fb[3];
-            q.vy = (T)fb[4];
-            q.e = (T)fb[5];
-            q.nut = (T)fb[6];
-            pack_cell<T>(q, u);
+            for (int k = 0; k < 5; ++k) sU[k * NL + w] = u[k];
+            sP[w] = q.p;
+            sQ[0 * NL + w] = q.vx;
+            sQ[1 * NL + w] = q.vy;
+            sQ[2 * NL + w] = q.t;
+            sQ[3 * NL + w] = q.nut;
         }
-        for (int k = 0; k < 5; ++k) sU[k * NL + w] = u[k];
-        sP[w] = q.p;
-        sQ[0 * NL + w] = q.vx;
-        sQ[1 * NL + w] = q.vy;
-        sQ[2 * NL + w] = q.t;
-        sQ[3 * NL + w] = q.nut;
+        JST_SYNC();
     }
-    JST_SYNC();
 
-    // ---- phase B1: pressure sensors (dissipation.rs:73-90) ---------------
+    // ---- B1: pressure sensors (dissipation.rs:73-90) ---------------------
     for (int w = tid; w < L::NSI; w += NT) {  // i-direction, rows i0-2 .. i0+TI+1
         int r = w / TJ, tj = w - r * TJ;
-        int li = r + 1, lj = tj + 3;
-        sSi[w] = pressure_sensor<T>(sP[(li - 1) * LJ + lj], sP[li * LJ + lj], sP[(li + 1) * LJ + lj]);
+        int o = (r + 1) * LJ + tj + 3;
+        sSi[w] = pressure_sensor<T>(sP[o - LJ], sP[o], sP[o + LJ]);
     }
     for (int w = tid; w < L::NSJ; w += NT) {  // j-direction, columns j0-2 .. j0+TJ+1
         int ti = w / (TJ + 4), cc = w - ti * (TJ + 4);
-        int li = ti + 3, lj = cc + 1;
-        sSj[w] = pressure_sensor<T>(sP[li * LJ + lj - 1], sP[li * LJ + lj], sP[li * LJ + lj + 1]);
+        int o = (ti + 3) * LJ + cc + 1;
+        sSj[w] = pressure_sensor<T>(sP[o - 1], sP[o], sP[o + 1]);
     }
 
-    // ---- phase B2: gradients + diffusion tensors on tile + ring ----------
+    // ---- B2: gradients, diffusion tensors (tile + ring), SA source (tile) -
     for (int w = tid; w < NR; w += NT) {
         int ri = w / RJ, rj = w - ri * RJ;
-        int gi = i0 - 1 + ri, gjr = j0 - 1 + rj;
+        int gi = i0 - 1 + ri;
         int li = ri + 2, lj = rj + 2;
         T g[8];
         if (gi >= ni) {
             for (int k = 0; k < 8; ++k) g[k] = T(0);  // far ghost ring (gradient.rs:96)
         } else {
-            // wall ghost ring takes the gradient of cell 0 (gradient.rs:93-95)
+            // the wall ghost ring takes cell 0's gradient with grad T = 0 (gradient.rs:93-95)
             int ci = gi < 0 ? 0 : gi;
             int cl = gi < 0 ? li + 1 : li;
-            int gj = wrapj(gjr, nj);
-            int jp = gj + 1 < nj ? gj + 1 : 0;
-            long up = (long)(ci + 1) * nj + gj, dn = (long)ci * nj + gj, lf = dn, rt = (long)ci * nj + jp;
-            T upx = (T)ld(I.tnx + up), upy = (T)ld(I.tny + up), dnx = (T)ld(I.tnx + dn), dny = (T)ld(I.tny + dn);
-            T lfx = (T)ld(I.nnx + lf), lfy = (T)ld(I.nny + lf), rtx = (T)ld(I.nnx + rt), rty = (T)ld(I.nny + rt);
-            T iv = (T)ld(I.inv_vol + dn);
+            int rt = ci - i0 + 1;  // geometry row of cell ci in the tau / n / ring boxes
+            int tdn = rt * L::GTJ + rj, tup = tdn + L::GTJ;
+            int nlf = rt * L::GNJ + rj, nrt = nlf + 1;
+            T upx = (T)gs[L::gTx + tup], upy = (T)gs[L::gTy + tup];
+            T dnx = (T)gs[L::gTx + tdn], dny = (T)gs[L::gTy + tdn];
+            T lfx = (T)gs[L::gNx + nlf], lfy = (T)gs[L::gNy + nlf];
+            T rtx = (T)gs[L::gNx + nrt], rty = (T)gs[L::gNy + nrt];
+            T iv = (T)gs[L::gIV + rt * RJ + rj];
             int o = cl * LJ + lj;
             for (int q = 0; q < 4; ++q) {
                 const T* f = sQ + q * NL;
@@ -437,114 +573,114 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
         sD[7 * NR + w] = d.dy4;
         if (ri >= 1 && ri <= TI && rj >= 1 && rj <= TJ) {
             int tcell = (ri - 1) * TJ + (rj - 1);
-            sG[0 * TI * TJ + tcell] = g[2];  // dvdx
-            sG[1 * TI * TJ + tcell] = g[1];  // dudy
-            sG[2 * TI * TJ + tcell] = g[6];  // dnutdx
-            sG[3 * TI * TJ + tcell] = g[7];  // dnutdy
-            sG[4 * TI * TJ + tcell] = d.chi;
-            sG[5 * TI * TJ + tcell] = d.fv1;
+            T s5 = sa_source<T>(sU[o], sU[4 * NL + o], (T)gs[L::gD2 + tcell], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
+            sS[tcell] = s5 * (T)gs[L::gV + tcell];
         }
     }
     JST_SYNC();
 
     const T half_cfl = (T)c.half_cfl, k2 = (T)c.k2, k4 = (T)c.k4, gm1 = (T)c.gm1;
 
-    // ---- phase C: net face fluxes G = conv - visc - diss -----------------
-    for (int w = tid; w < L::NFT; w += NT) {  // tau faces i0 .. i0+TI
-        int r = w / TJ, tj = w - r * TJ;
-        int f = i0 + r, gj = j0 + tj;
-        if (f > ni || gj >= nj) continue;
-        long fid = (long)f * nj + gj;
-        T nx = (T)ld(I.tnx + fid), ny = (T)ld(I.tny + fid);
-        int lo = (r + 3) * LJ + (tj + 3);  // cell f (cell f-1 is lo - LJ)
-        T fu[5], cv[5];
-        for (int k = 0; k < 5; ++k) fu[k] = T(0.5) * (sU[k * NL + lo - LJ] + sU[k * NL + lo]);
-        euler_flux<T>(fu, nx, ny, gm1, cv);
-        int da = r * RJ + (tj + 1), db = da + RJ;  // D of cells f-1, f
-        T hx = T(0.5) * nx, hy = T(0.5) * ny;
-        int a = f < ni - 1 ? f : ni - 1, b = f - 1 > 0 ? f - 1 : 0;
-        if (a < 0) a = 0;
-        if (b > ni - 1) b = ni - 1;
-        T lam = half_cfl * (ld(ratio + (long)a * nj + gj) + ld(ratio + (long)b * nj + gj));
-        T m = tmax<T>(tmax<T>(tmax<T>(sSi[r * TJ + tj], sSi[(r + 1) * TJ + tj]), sSi[(r + 2) * TJ + tj]),
-                      sSi[(r + 3) * TJ + tj]);
-        T e2 = k2 * m, e4 = tmax<T>(k4 - e2, T(0));
-        for (int k = 0; k < 5; ++k) {
-            const T* U = sU + k * NL;
-            T d1 = U[lo] - U[lo - LJ];
-            T d3 = U[lo + LJ] - T(3) * U[lo] + T(3) * U[lo - LJ] - U[lo - 2 * LJ];
-            T vis = T(0);
-            if (k > 0)
-                vis = (sD[(k - 1) * NR + da] + sD[(k - 1) * NR + db]) * hx +
-                      (sD[(k + 3) * NR + da] + sD[(k + 3) * NR + db]) * hy;
-            sFt[k * L::NFT + w] = cv[k] - vis - lam * (d1 * e2 - d3 * e4);
+    // ---- C: net face fluxes G = conv - visc - diss, each face once -------
+    T* sFt = sm + L::oX;               // tau faces i0 .. i0+TI (aliases the dead P, Q)
+    T* sFn = sFt + 5 * L::NFT;         // n faces j0 .. j0+TJ
+    for (int w = tid; w < L::NFT + L::NFN; w += NT) {
+        T nx, ny, lam, e2, e4;
+        int lo, step, da, db;
+        bool tau = w < L::NFT;
+        if (tau) {
+            int r = w / TJ, tj = w - r * TJ;
+            int f = i0 + r, gj = j0 + tj;
+            if (f > ni || gj >= nj) continue;
+            int gt = (r + 1) * L::GTJ + tj + 1;
+            nx = (T)gs[L::gTx + gt];
+            ny = (T)gs[L::gTy + gt];
+            lo = (r + 3) * LJ + (tj + 3);  // cell f; cell f-1 is lo - LJ
+            step = LJ;
+            da = r * RJ + (tj + 1);        // ring cells f-1, f
+            db = da + RJ;
+            T m = tmax<T>(tmax<T>(tmax<T>(sSi[r * TJ + tj], sSi[(r + 1) * TJ + tj]), sSi[(r + 2) * TJ + tj]),
+                          sSi[(r + 3) * TJ + tj]);
+            e2 = k2 * m;
+        } else {
+            int v = w - L::NFT;
+            int ti = v / (TJ + 1), cc = v - ti * (TJ + 1);
+            int gi = i0 + ti, jf = j0 + cc;
+            if (gi >= ni || jf > nj) continue;
+            int gn = (ti + 1) * L::GNJ + cc + 1;
+            nx = (T)gs[L::gNx + gn];
+            ny = (T)gs[L::gNy + gn];
+            lo = (ti + 3) * LJ + (cc + 3);  // cell jf; cell jf-1 is lo - 1
+            step = 1;
+            db = (ti + 1) * RJ + (cc + 1);
+            da = db - 1;
+            const T* S = sSj + ti * (TJ + 4) + cc;
+            T m = tmax<T>(tmax<T>(tmax<T>(S[0], S[1]), S[2]), S[3]);
+            e2 = k2 * m;
         }
-    }
-    for (int w = tid; w < L::NFN; w += NT) {  // n faces j0 .. j0+TJ
-        int ti = w / (TJ + 1), cc = w - ti * (TJ + 1);
-        int gi = i0 + ti, jf = j0 + cc;
-        if (gi >= ni || jf > nj) continue;
-        int jw = jf >= nj ? jf - nj : jf;
-        int jm = jw > 0 ? jw - 1 : nj - 1;
-        long fid = (long)gi * nj + jw;
-        T nx = (T)ld(I.nnx + fid), ny = (T)ld(I.nny + fid);
-        int lo = (ti + 3) * LJ + (cc + 3);  // cell jf (cell jf-1 is lo - 1)
+        e4 = tmax<T>(k4 - e2, T(0));
+        lam = half_cfl * (sRat[db] + sRat[da]);
         T fu[5], cv[5];
-        for (int k = 0; k < 5; ++k) fu[k] = T(0.5) * (sU[k * NL + lo - 1] + sU[k * NL + lo]);
+        for (int k = 0; k < 5; ++k) fu[k] = T(0.5) * (sU[k * NL + lo - step] + sU[k * NL + lo]);
         euler_flux<T>(fu, nx, ny, gm1, cv);
-        int db = (ti + 1) * RJ + (cc + 1), da = db - 1;
         T hx = T(0.5) * nx, hy = T(0.5) * ny;
-        T lam = half_cfl * (ld(ratio + fid) + ld(ratio + (long)gi * nj + jm));
-        const T* S = sSj + ti * (TJ + 4) + cc;
-        T m = tmax<T>(tmax<T>(tmax<T>(S[0], S[1]), S[2]), S[3]);
-        T e2 = k2 * m, e4 = tmax<T>(k4 - e2, T(0));
+        T* out = tau ? sFt + w : sFn + (w - L::NFT);
+        const int ostride = tau ? L::NFT : L::NFN;
         for (int k = 0; k < 5; ++k) {
             const T* U = sU + k * NL;
-            T d1 = U[lo] - U[lo - 1];
-            T d3 = U[lo + 1] - T(3) * U[lo] + T(3) * U[lo - 1] - U[lo - 2];
+            T d1 = U[lo] - U[lo - step];
+            T d3 = U[lo + step] - T(3) * U[lo] + T(3) * U[lo - step] - U[lo - 2 * step];
             T vis = T(0);
             if (k > 0)
                 vis = (sD[(k - 1) * NR + da] + sD[(k - 1) * NR + db]) * hx +
                       (sD[(k + 3) * NR + da] + sD[(k + 3) * NR + db]) * hy;
-            sFn[k * L::NFN + w] = cv[k] - vis - lam * (d1 * e2 - d3 * e4);
+            out[k * ostride] = cv[k] - vis - lam * (d1 * e2 - d3 * e4);
         }
     }
     JST_SYNC();
 
-    // ---- phase D: source, RK update, unpack check, last-stage epilogue ---
+    // ---- D: RK update, unpack check, last-stage epilogue -----------------
     double mloc = __longlong_as_double(0x7ff0000000000000LL);
     double sres = 0.0;
-    for (int w = tid; w < TI * TJ; w += NT) {
+    for (int w = tid; w < TT; w += NT) {
         int ti = w / TJ, tj = w - ti * TJ;
         int gi = i0 + ti, gj = j0 + tj;
         if (gi >= ni || gj >= nj) continue;
         long id = (long)gi * nj + gj;
-        int lo = (ti + 3) * LJ + (tj + 3);
-        T src5 = sa_source<T>(sU[lo], sU[4 * NL + lo], (T)ld(I.inv_d2 + id), sG[4 * TI * TJ + w],
-                              sG[5 * TI * TJ + w], sG[0 * TI * TJ + w], sG[1 * TI * TJ + w], sG[2 * TI * TJ + w],
-                              sG[3 * TI * TJ + w], c) *
-                 (T)ld(I.vol + id);
+        double uo[5];
+        for (int k = 0; k < 5; ++k) uo[k] = gs[L::gUn + k * TT + w];
         T R[5];
+        const int fd = ti * (TJ + 1) + tj;
         for (int k = 0; k < 5; ++k)
-            R[k] = (sFt[k * L::NFT + w + TJ] - sFt[k * L::NFT + w]) +
-                   (sFn[k * L::NFN + ti * (TJ + 1) + tj + 1] - sFn[k * L::NFN + ti * (TJ + 1) + tj]);
-        R[4] -= src5;
+            R[k] = (sFt[k * L::NFT + w + TJ] - sFt[k * L::NFT + w]) + (sFn[k * L::NFN + fd + 1] - sFn[k * L::NFN + fd]);
+        R[4] -= sS[w];
+        int rc = (ti + 1) * RJ + tj + 1;  // ring index of the cell
         double a = alpha * (I.local_dt ? ld(I.ldt + id) : I.st->dt);
-        double sc = a * ld(I.inv_vol + id);
-        double uo[5], un[5];
-        for (int k = 0; k < 5; ++k) uo[k] = I.un[k][id];
+        double sc = a * gs[L::gIV + rc];
+        double un[5];
         for (int k = 0; k < 5; ++k) {
             if (sizeof(T) == sizeof(double)) un[k] = uo[k] - (double)R[k] * sc;
             else un[k] = uo[k] - (double)(R[k] * (T)sc);  // FP32 increment, FP64 accumulator
             dst[k][id] = (TD)un[k];
         }
-        // unpack checks (solver.rs:160-171)
-        double rho = un[0];
-        bool bad = isnan(rho) || rho <= 1e-15;
+        // unpack checks (solver.rs:160-171), on the stored precision
+        bool bad;
         Prim<double> q{};
-        if (!bad) {
-            q = unpack_cell<double>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
-            bad = isnan(q.p) || q.p <= 1e-15;
+        if (LAST || sizeof(T) == sizeof(double)) {
+            double rho = un[0];
+            bad = isnan(rho) || rho <= 1e-15;
+            if (!bad) {
+                q = unpack_cell<double>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
+                bad = isnan(q.p) || q.p <= 1e-15;
+            }
+        } else {
+            T rho = (T)un[0];
+            bad = isnan(rho) || rho <= T(1e-15);
+            if (!bad) {
+                T inv = T(1) / rho, vx = (T)un[1] * inv, vy = (T)un[2] * inv;
+                T p = (T)c.gm1 * ((T)un[3] - rho * (vx * vx + vy * vy) * T(0.5));
+                bad = isnan(p) || p <= T(1e-15);
+            }
         }
         if (bad) {
             atomicMin(&I.st->bad, (stage_id << 32) | (unsigned long long)id);
@@ -553,8 +689,16 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
         if (LAST) {
             double d = un[0] - uo[0];  // solver.rs:195
             sres += d * d;
-            double dl = cell_localdt<T>(I, gi, gj, q.vx, q.vy, q.t);
-            ratio_next[id] = (T)(ld(I.vol + id) / dl);
+            // timestep.rs:30-42 from the staged geometry
+            int tdn = (ti + 1) * L::GTJ + tj + 1, tup = tdn + L::GTJ;
+            int nlf = (ti + 1) * L::GNJ + tj + 1, nrt = nlf + 1;
+            double aa = 0.5 * (gs[L::gTx + tdn] + gs[L::gTx + tup]);
+            double bb = 0.5 * (gs[L::gTy + tdn] + gs[L::gTy + tup]);
+            double cc = 0.5 * (gs[L::gNx + nlf] + gs[L::gNx + nrt]);
+            double dd = 0.5 * (gs[L::gNy + nlf] + gs[L::gNy + nrt]);
+            double vol = gs[L::gV + w];
+            double dl = local_dt<double>(q.vx, q.vy, sqrt(c.rg * q.t), aa, bb, cc, dd, c.cfl * vol);
+            ratio_next[id] = (T)(vol / dl);
             if (I.local_dt) I.ldt[id] = dl;
             mloc = fmin(mloc, dl);
         }
