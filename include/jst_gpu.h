@@ -193,6 +193,22 @@ jst_status jst_write_csv(jst_solver* s, const char* path);
  * and stage_ms[0..4] receive the five stage kernels' times. */
 jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_ms);
 
+/* The density residual of solver.rs:190-200, sqrt(sum((rho - rho_prev)^2) / NI / NJ),
+ * for callers that cannot allocate device memory (no counterpart in the
+ * reference, whose Solver owns its fields).  Plugin hosts that own every
+ * device allocation through their own pool, and monitoring loops that must
+ * not call cudaMalloc (it synchronises the device), pass device pointers to
+ * their own NI*NJ density fields and to one double for the result; the call
+ * enqueues two kernels on `stream` (a cudaStream_t, NULL for the default
+ * stream) and returns without synchronising or allocating.  Its scratch is a
+ * fixed file-scope device array of 8192 partial sums, so NI*NJ may not exceed
+ * 16,777,216 cells (larger sizes fail with JST_ERR_ARG before any launch).
+ * The first call on a device looks up that array's address; make it before
+ * any stream capture.  All calls share the array: calls whose kernels overlap
+ * on the GPU race, so serialise them (one stream, or events). */
+jst_status jst_residual_noalloc(const double* rho, const double* rho_prev, int ni, int nj, double* out,
+                                void* stream);
+
 /* Version string of this library. */
 const char* jst_version(void);
 

@@ -33,6 +33,7 @@ UNITS = {
     "passes.cu": ["--fmad=false"],
     "fused.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "api.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -30,6 +30,9 @@ static thread_local std::string g_create_error;
 
 namespace jst {
 
+// Error text for entry points without a handle (read with jst_last_error(NULL)).
+void set_call_error(const std::string& msg) { g_create_error = msg; }
+
 const double RK_ALPHA[5] = {0.25, 1.0 / 6.0, 0.375, 0.5, 1.0};  // config.rs:295
 
 // Config::finish (config.rs:251-284) + the constant sub-expressions of

@@ -42,7 +42,7 @@ FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
 EXPORTS = ["jst_default_opts", "jst_create_from_paths", "jst_create", "jst_destroy", "jst_last_error", "jst_ni",
            "jst_nj", "jst_advance", "jst_run", "jst_residual_terms", "jst_timestep", "jst_residual",
            "jst_totaltime", "jst_step_count", "jst_get_field", "jst_get_faces", "jst_set_conserved",
-           "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps"]
+           "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps", "jst_residual_noalloc"]
 
 
 class Opts(C.Structure):
@@ -118,6 +118,7 @@ def lib() -> C.CDLL:
         L.jst_write_csv.argtypes = [vp, C.c_char_p]
         L.jst_version.restype = C.c_char_p
         L.jst_time_steps.argtypes = [vp, i, pd, pd]
+        L.jst_residual_noalloc.argtypes = [vp, vp, i, i, vp, vp]
         L.jst_debug_set_uniform.argtypes = [vp, d, d, d, d, d]
         L.jst_debug_kernel.argtypes = [vp, C.c_char_p]
         _lib = L
