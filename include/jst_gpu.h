@@ -193,6 +193,66 @@ jst_status jst_write_csv(jst_solver* s, const char* path);
  * and stage_ms[0..4] receive the five stage kernels' times. */
 jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_ms);
 
+/* ------------------------------------------------------------------------
+ * Batched solving and serving (no counterpart in the reference, which solves
+ * one case per process): many independent solves of different meshes and
+ * flow conditions share one persistent stage kernel over a table of
+ * (instance, tile) work items, with each RK step replayed from a CUDA graph.
+ * Instances are admitted as HBM and slots allow, stay device-resident, and
+ * retire individually on convergence, on NonPhysical, or at their step limit.
+ * ------------------------------------------------------------------------ */
+typedef struct jst_batch jst_batch;
+
+typedef struct {
+    int precision;        /* jst_precision of every instance */
+    int dt_mode;          /* jst_dt_mode of every instance */
+    int device;
+    int tile_i, tile_j;   /* 0 = default tile */
+    int max_instances;    /* slots */
+    int steps_per_poll;   /* RK steps per graph replay between convergence polls */
+    double hbm_budget_gb; /* device memory the batch may hold for instances */
+    int keep_fields;      /* copy U of retired instances to host memory */
+} jst_batch_opts;
+
+void jst_batch_default_opts(jst_batch_opts* o);
+jst_status jst_batch_create(const jst_batch_opts* o, jst_batch** out);
+void jst_batch_destroy(jst_batch* b);
+
+/* Queue one solve.  max_steps < 0 uses the config's solver.iteration;
+ * residual_drop > 0 retires the instance once its residual falls below
+ * residual_drop times its first-step residual (the config's targetres also
+ * applies); cl_tol > 0 retires it once |CL(n) - CL(n-100)| < cl_tol.  The
+ * instance is admitted at the next jst_batch_step when a slot and memory are
+ * free.  *id receives its id. */
+jst_status jst_batch_submit(jst_batch* b, const char* config_json, const double* xy, int n_rings, int n_theta,
+                            int64_t max_steps, double residual_drop, double cl_tol, int64_t* id);
+
+/* Admit queued instances, advance every active instance by up to nsteps RK
+ * steps (in graph replays of steps_per_poll), retire finished ones.  Returns
+ * after nsteps or when nothing is active or queued. */
+jst_status jst_batch_step(jst_batch* b, int nsteps);
+
+/* Counts of active and queued instances and device bytes in use. */
+jst_status jst_batch_stats(jst_batch* b, int* active, int* queued, double* bytes_in_use);
+
+/* Ids retired since the last poll (up to cap); *n receives the count. */
+jst_status jst_batch_poll(jst_batch* b, int64_t* ids, int cap, int* n);
+
+typedef struct {
+    int64_t id;
+    int status;        /* JST_OK, JST_ERR_NONPHYSICAL, or JST_ERR_TIMEOUT (step limit) */
+    int64_t steps;
+    double residual, residual_first, totaltime;
+    double cl, cd;
+    double t_submit, t_admit, t_done; /* seconds since the batch was created */
+    int ni, nj;
+    jst_nonphysical bad;
+} jst_batch_result;
+
+/* Result of a retired instance; with keep_fields, fields (5*NI*NJ doubles,
+ * may be NULL) receives its final conserved state. */
+jst_status jst_batch_result_get(jst_batch* b, int64_t id, jst_batch_result* r, double* fields, size_t n);
+
 /* The density residual of solver.rs:190-200, sqrt(sum((rho - rho_prev)^2) / NI / NJ),
  * for callers that cannot allocate device memory (no counterpart in the
  * reference, whose Solver owns its fields).  Plugin hosts that own every

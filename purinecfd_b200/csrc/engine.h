@@ -33,6 +33,9 @@ struct SolverCore {
 };
 
 void nonphysical_report(const PhysConst& c, long i, long j, const double u[5], jst_nonphysical* bad);
+struct RawConfig;
+PhysConst make_phys(const RawConfig& r);
+void set_call_error(const std::string& msg);
 
 class Engine {
   public:

@@ -14,6 +14,11 @@
 #include <type_traits>
 #include <vector>
 
+#include <chrono>
+#include <deque>
+#include <map>
+
+#include "config_mesh.h"
 #include "engine.h"
 #include "fused_kernels.cuh"
 
@@ -63,7 +68,12 @@ __global__ void k_far_geom(Geom g, double* far) {
 // through tau face (0, j) exactly as the residual terms form them
 // (boundary.rs:30-51 mirror ghost, gradient.rs:22-35 and 87-95, viscous.rs:37-71
 // and 128-139).  One block, fixed-order reduction.
-__global__ void k_wall_force(Geom g, const double* const* un, PhysConst c, int fresh, double* out) {
+struct UnPtrs {
+    const double* u[5];
+};
+
+__global__ void k_wall_force(Geom g, UnPtrs un_p, PhysConst c, int fresh, double* out) {
+    const double* const* un = un_p.u;
     __shared__ double rx[256], ry[256];
     int nj = g.nj;
     double ax = 0.0, ay = 0.0;
@@ -126,14 +136,16 @@ __global__ void k_wall_force(Geom g, const double* const* un, PhysConst c, int f
     }
 }
 
-template <class T> size_t stage_smem(int ti, int tj);
+void launch_wall_force(const Geom& g, const UnPtrs& up, const PhysConst& c, double* out, cudaStream_t st) {
+    JST_LAUNCH(k_wall_force, 1, 256, 0, st, g, up, c, 0, out);
+}
 
 // Tile configurations compiled into the library: (TI, TJ, NT).
 #define JST_FOR_TILES(X) X(4, 32, 256) X(8, 32, 256) X(16, 32, 256) X(4, 64, 256) X(8, 64, 256)
 
 template <class T> struct Kernels {
-    void (*stage[3])(const TileRef*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};  // first, mid, last
-    void (*step_dt)(const TileRef*, const Inst<T>*, int, int) = nullptr;
+    void (*stage[3])(const TileRef*, const int*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};
+    void (*step_dt)(const TileRef*, const int*, const Inst<T>*, int, int) = nullptr;
     size_t smem = 0;
     int nt = 256;
 };
@@ -223,6 +235,7 @@ template <class T> class FusedEngine : public Engine {
         size_t o_inst = add(sizeof(Inst<T>));
         size_t o_tiles = add(tiles.size() * sizeof(TileRef));
         size_t o_force = add(8 * sizeof(double));
+        size_t o_ntiles = add(sizeof(int));
         size_t o_unptr = add(5 * sizeof(double*));
         hist_cap_ = 4096;
         size_t o_hist = add(hist_cap_ * sizeof(double));
@@ -261,9 +274,11 @@ template <class T> class FusedEngine : public Engine {
         d_inst_ = reinterpret_cast<Inst<T>*>(base + o_inst);
         d_tiles_ = reinterpret_cast<TileRef*>(base + o_tiles);
         d_force_ = reinterpret_cast<double*>(base + o_force);
+        d_ntiles_ = reinterpret_cast<int*>(base + o_ntiles);
         d_unptr_ = reinterpret_cast<double**>(base + o_unptr);
         cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, C.st);
+        cudaMemcpyAsync(d_ntiles_, &ntiles_, sizeof(int), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_unptr_, inst_.un, 5 * sizeof(double*), cudaMemcpyHostToDevice, C.st);
         if (cudaMallocHost(&h_state_, sizeof(InstState)) != cudaSuccess) {
             err = "cudaMallocHost failed";
@@ -285,7 +300,10 @@ template <class T> class FusedEngine : public Engine {
         s.fresh = fresh;
         s.done = 0;
         s.max_step = INT_MAX;
+        s.drop = 0.0;
+        s.res_first = 0.0;
         cudaMemcpyAsync(inst_.st, &s, sizeof s, cudaMemcpyHostToDevice, core_->st);
+        cudaStreamSynchronize(core_->st);
     }
 
     void init() override {
@@ -298,13 +316,13 @@ template <class T> class FusedEngine : public Engine {
     }
 
     void launch_step_dt() {
-        JST_LAUNCH(K_.step_dt, ntiles_, K_.nt, 0, core_->st, d_tiles_, d_inst_, ti_, tj_);
+        JST_LAUNCH(K_.step_dt, ntiles_, K_.nt, 0, core_->st, d_tiles_, d_ntiles_, d_inst_, ti_, tj_);
     }
 
     void enqueue_step(cudaStream_t st) {
         for (int s = 0; s < 5; ++s) {
             auto kern = s == 0 ? K_.stage[0] : (s == 4 ? K_.stage[2] : K_.stage[1]);
-            JST_LAUNCH(kern, ntiles_, K_.nt, K_.smem, st, d_tiles_, d_inst_, s, RK_ALPHA[s]);
+            JST_LAUNCH(kern, ntiles_, K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, s, RK_ALPHA[s]);
         }
     }
 
@@ -516,8 +534,9 @@ template <class T> class FusedEngine : public Engine {
     jst_status wall_force(double* fx, double* fy) override {
         InstState s;
         if (read_state(&s) != JST_OK) return JST_ERR_CUDA;
-        JST_LAUNCH(k_wall_force, 1, 256, 0, core_->st, core_->g, (const double* const*)d_unptr_, core_->c, s.fresh,
-                   d_force_);
+        UnPtrs up;
+        for (int k = 0; k < 5; ++k) up.u[k] = inst_.un[k];
+        JST_LAUNCH(k_wall_force, 1, 256, 0, core_->st, core_->g, up, core_->c, s.fresh, d_force_);
         double f[2];
         cudaMemcpyAsync(f, d_force_, sizeof f, cudaMemcpyDeviceToHost, core_->st);
         if (cudaStreamSynchronize(core_->st) != cudaSuccess) return JST_ERR_CUDA;
@@ -565,7 +584,7 @@ template <class T> class FusedEngine : public Engine {
             cudaEventRecord(ev[2], st);
             for (int q = 0; q < 5; ++q) {
                 auto kern = q == 0 ? K_.stage[0] : (q == 4 ? K_.stage[2] : K_.stage[1]);
-                JST_LAUNCH(kern, ntiles_, K_.nt, K_.smem, st, d_tiles_, d_inst_, q, RK_ALPHA[q]);
+                JST_LAUNCH(kern, ntiles_, K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, q, RK_ALPHA[q]);
                 cudaEventRecord(ev[3 + q], st);
             }
         }
@@ -597,10 +616,658 @@ template <class T> class FusedEngine : public Engine {
     Inst<T>* d_inst_ = nullptr;
     TileRef* d_tiles_ = nullptr;
     double* d_force_ = nullptr;
+    int* d_ntiles_ = nullptr;
     double** d_unptr_ = nullptr;
     InstState* h_state_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
 };
+
+// ------------------------------------------------------------------ batch ----
+// Many independent solves in one persistent stage kernel.  Each instance owns
+// a block of a pre-allocated HBM arena (geometry, state, per-tile partials),
+// a slot in the device instance table and its tiles in the device tile
+// table; the stage kernels read the table size from device memory, so the
+// captured graph of K RK steps stays valid while instances come and go.
+
+namespace {
+
+// First-fit allocator over one cudaMalloc'd arena (offsets in bytes).
+struct Arena {
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+    std::map<size_t, size_t> free_;  // offset -> size
+    static size_t round(size_t n) { return (n + 255) / 256 * 256; }
+    bool init(size_t bytes) {
+        cap = round(bytes);
+        if (cudaMalloc(&base, cap) != cudaSuccess) return false;
+        free_[0] = cap;
+        return true;
+    }
+    bool alloc(size_t n, size_t* off) {
+        n = round(n);
+        for (auto it = free_.begin(); it != free_.end(); ++it)
+            if (it->second >= n) {
+                *off = it->first;
+                size_t rem = it->second - n, o2 = it->first + n;
+                free_.erase(it);
+                if (rem) free_[o2] = rem;
+                used += n;
+                return true;
+            }
+        return false;
+    }
+    void release(size_t off, size_t n) {
+        n = round(n);
+        used -= n;
+        auto it = free_.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    ~Arena() {
+        if (base) cudaFree(base);
+    }
+};
+
+using Clock = std::chrono::steady_clock;
+
+}  // namespace
+
+struct BatchResultFull {
+    jst_batch_result r{};
+    std::vector<double> fields;
+};
+
+class BatchBase {
+  public:
+    virtual ~BatchBase() {}
+    virtual jst_status submit(const char* cfg, const double* xy, int nr, int nt, int64_t max_steps, double drop,
+                              double cl_tol, int64_t* id) = 0;
+    virtual jst_status step(int nsteps) = 0;
+    virtual void stats(int* active, int* queued, double* bytes) = 0;
+    virtual int poll(int64_t* ids, int cap) = 0;
+    virtual bool result(int64_t id, BatchResultFull** out) = 0;
+};
+
+template <class T> class Batch : public BatchBase {
+    struct Pending {
+        int64_t id;
+        RawConfig raw;
+        std::vector<double> xy;
+        int n_rings, n_theta;
+        int64_t max_steps;
+        double drop, cl_tol, t_submit;
+    };
+    struct Slot {
+        bool used = false;
+        int64_t id = -1;
+        size_t off = 0, bytes = 0;
+        int ni = 0, nj = 0, ntiles = 0;
+        int64_t max_steps = 0;
+        double drop = 0, cl_tol = 0, t_submit = 0, t_admit = 0;
+        double chord = 1, aoa = 0;
+        Geom g{};
+        std::vector<std::pair<int, double>> cl_hist;
+    };
+
+  public:
+    explicit Batch(const jst_batch_opts& o) : o_(o) { t0_ = Clock::now(); }
+    ~Batch() override {
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (small_) cudaFree(small_);
+        if (h_states_) cudaFreeHost(h_states_);
+        if (st_) cudaStreamDestroy(st_);
+    }
+
+    bool create(std::string& err) {
+        if (cudaSetDevice(o_.device) != cudaSuccess) {
+            err = "cudaSetDevice failed";
+            return false;
+        }
+        cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
+        int ti = o_.tile_i, tj = o_.tile_j;
+        if (ti <= 0 || tj <= 0) default_tile(o_.precision, 128, &ti, &tj);
+        if (!pick_kernels<T>(ti, tj, &K_)) {
+            err = "unsupported tile shape";
+            return false;
+        }
+        ti_ = ti;
+        tj_ = tj;
+        for (int k = 0; k < 3; ++k)
+            if (cudaFuncSetAttribute(K_.stage[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K_.smem) !=
+                cudaSuccess) {
+                err = "stage kernel shared memory too large";
+                return false;
+            }
+        int sms = 0, occ = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o_.device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K_.stage[1], K_.nt, K_.smem);
+        grid_ = std::max(1, sms * std::max(1, occ));
+        nslots_ = std::max(1, o_.max_instances);
+        max_tiles_ = 1 << 22;
+        size_t bytes = nslots_ * (sizeof(Inst<T>) + sizeof(InstState) + sizeof(int) + 2 * sizeof(double)) +
+                       (size_t)max_tiles_ * sizeof(TileRef) + 4096;
+        if (cudaMalloc(&small_, bytes) != cudaSuccess) {
+            err = "cudaMalloc failed for the batch tables";
+            return false;
+        }
+        cudaMemset(small_, 0, bytes);
+        char* q = static_cast<char*>(small_);
+        d_insts_ = reinterpret_cast<Inst<T>*>(q);
+        q += nslots_ * sizeof(Inst<T>);
+        d_states_ = reinterpret_cast<InstState*>(q);
+        q += nslots_ * sizeof(InstState);
+        d_force_ = reinterpret_cast<double*>(q);
+        q += nslots_ * 2 * sizeof(double);
+        d_counts_ = reinterpret_cast<int*>(q);
+        q += nslots_ * sizeof(int);
+        q = reinterpret_cast<char*>(((uintptr_t)q + 255) / 256 * 256);
+        d_ntiles_ = reinterpret_cast<int*>(q);
+        q += 256;
+        d_tiles_ = reinterpret_cast<TileRef*>(q);
+        if (cudaMallocHost(&h_states_, nslots_ * sizeof(InstState)) != cudaSuccess) {
+            err = "cudaMallocHost failed";
+            return false;
+        }
+        h_insts_.assign(nslots_, Inst<T>{});
+        slots_.assign(nslots_, Slot{});
+        size_t budget = (size_t)(o_.hbm_budget_gb * 1e9);
+        if (budget == 0) {
+            size_t fr = 0, tot = 0;
+            cudaMemGetInfo(&fr, &tot);
+            budget = (size_t)(0.5 * fr);
+        }
+        if (!arena_.init(budget)) {
+            err = "cudaMalloc failed for the instance arena";
+            return false;
+        }
+        int zero = 0;
+        cudaMemcpy(d_ntiles_, &zero, sizeof zero, cudaMemcpyHostToDevice);
+        return true;
+    }
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0_).count(); }
+
+    jst_status submit(const char* cfg, const double* xy, int nr, int nt, int64_t max_steps, double drop,
+                      double cl_tol, int64_t* id) override {
+        Pending p;
+        std::string err;
+        if (!parse_config(cfg, p.raw, err)) {
+            set_call_error(err);
+            return JST_ERR_CONFIG;
+        }
+        if (p.raw.halo < 3) {
+            set_call_error("simulation.IM must be >= 3");
+            return JST_ERR_CONFIG;
+        }
+        p.xy.assign(xy, xy + 2 * (size_t)nr * nt);
+        // trim_closing_duplicate (mesh.rs:169-189)
+        bool closed = nt >= 2;
+        for (int r = 0; r < nr && closed; ++r)
+            closed = std::fabs(p.xy[2 * ((size_t)r * nt)] - p.xy[2 * ((size_t)r * nt + nt - 1)]) <= 1e-10 &&
+                     std::fabs(p.xy[2 * ((size_t)r * nt) + 1] - p.xy[2 * ((size_t)r * nt + nt - 1) + 1]) <= 1e-10;
+        if (closed) {
+            std::vector<double> t(2 * (size_t)nr * (nt - 1));
+            for (int r = 0; r < nr; ++r)
+                std::memcpy(&t[2 * (size_t)r * (nt - 1)], &p.xy[2 * (size_t)r * nt], sizeof(double) * 2 * (nt - 1));
+            p.xy.swap(t);
+            nt -= 1;
+        }
+        if (nr < 4 || nt < 8) {
+            set_call_error("mesh too small");
+            return JST_ERR_MESH_TOO_SMALL;
+        }
+        p.n_rings = nr;
+        p.n_theta = nt;
+        p.max_steps = max_steps < 0 ? p.raw.iteration : max_steps;
+        p.drop = drop;
+        p.cl_tol = cl_tol;
+        p.t_submit = now();
+        p.id = next_id_++;
+        *id = p.id;
+        queue_.push_back(std::move(p));
+        return JST_OK;
+    }
+
+    size_t instance_bytes(int nr, int nt, int ntiles) const {
+        size_t n = (size_t)(nr - 1) * nt, ntau = (size_t)nr * nt;
+        size_t b = 0;
+        auto add = [&](size_t x) { b += (x + 255) / 256 * 256; };
+        add((10 * n + 4 * ntau) * sizeof(double));  // geometry
+        add(2 * (size_t)nr * nt * sizeof(double));  // nodes
+        add(5 * n * sizeof(double));                 // U_n
+        add(10 * n * sizeof(T));                     // U_a, U_b
+        add(2 * n * sizeof(T));                      // ratio
+        add(n * sizeof(double));                     // localdt
+        add(2 * (size_t)ntiles * sizeof(double));    // partials
+        add(5 * (size_t)nt * sizeof(double));        // far
+        return b;
+    }
+
+    // Admit queued instances while a slot and arena memory are free.
+    jst_status admit() {
+        bool changed = false;
+        while (!queue_.empty()) {
+            int slot = -1;
+            for (int k = 0; k < nslots_; ++k)
+                if (!slots_[k].used) {
+                    slot = k;
+                    break;
+                }
+            if (slot < 0) break;
+            Pending& p = queue_.front();
+            int ni = p.n_rings - 1, nj = p.n_theta;
+            int tiles_i = (ni + ti_ - 1) / ti_, tiles_j = (nj + tj_ - 1) / tj_, ntl = tiles_i * tiles_j;
+            if ((long)h_tiles_.size() + ntl > max_tiles_) break;
+            size_t bytes = instance_bytes(p.n_rings, p.n_theta, ntl), off = 0;
+            if (!arena_.alloc(bytes, &off)) break;
+            Slot& S = slots_[slot];
+            S = Slot{};
+            S.used = true;
+            S.id = p.id;
+            S.off = off;
+            S.bytes = bytes;
+            S.ni = ni;
+            S.nj = nj;
+            S.ntiles = ntl;
+            S.max_steps = p.max_steps;
+            S.drop = p.drop;
+            S.cl_tol = p.cl_tol;
+            S.t_submit = p.t_submit;
+            S.t_admit = now();
+            S.aoa = p.raw.aoa * (M_PI / 180.0);
+            double xmin = 1e300, xmax = -1e300;
+            for (int t = 0; t < nj; ++t) {
+                xmin = std::min(xmin, p.xy[2 * t]);
+                xmax = std::max(xmax, p.xy[2 * t]);
+            }
+            S.chord = p.raw.chord > 0 ? p.raw.chord : xmax - xmin;
+            PhysConst c = make_phys(p.raw);
+            size_t n = (size_t)ni * nj, ntau = (size_t)(ni + 1) * nj;
+            char* q = arena_.base + off;
+            auto take = [&](size_t bytes_) {
+                char* r = q;
+                q += (bytes_ + 255) / 256 * 256;
+                return r;
+            };
+            double* geo = reinterpret_cast<double*>(take((10 * n + 4 * ntau) * sizeof(double)));
+            Geom& g = S.g;
+            g.ni = ni;
+            g.nj = nj;
+            double* gq = geo;
+            g.vol = gq; gq += n;
+            g.cx = gq; gq += n;
+            g.cy = gq; gq += n;
+            g.wdist = gq; gq += n;
+            g.inv_vol = gq; gq += n;
+            g.inv_d2 = gq; gq += n;
+            g.tnx = gq; gq += ntau;
+            g.tny = gq; gq += ntau;
+            g.tmx = gq; gq += ntau;
+            g.tmy = gq; gq += ntau;
+            g.nnx = gq; gq += n;
+            g.nny = gq; gq += n;
+            g.nmx = gq; gq += n;
+            g.nmy = gq; gq += n;
+            double* d_xy = reinterpret_cast<double*>(take(2 * (size_t)p.n_rings * nj * sizeof(double)));
+            Inst<T>& I = h_insts_[slot];
+            I = Inst<T>{};
+            I.ni = ni;
+            I.nj = nj;
+            I.ntiles = ntl;
+            I.local_dt = o_.dt_mode == JST_DT_LOCAL;
+            I.tnx = g.tnx;
+            I.tny = g.tny;
+            I.nnx = g.nnx;
+            I.nny = g.nny;
+            I.vol = g.vol;
+            I.inv_vol = g.inv_vol;
+            I.inv_d2 = g.inv_d2;
+            double* un = reinterpret_cast<double*>(take(5 * n * sizeof(double)));
+            T* ua = reinterpret_cast<T*>(take(10 * n * sizeof(T)));
+            T* ra = reinterpret_cast<T*>(take(2 * n * sizeof(T)));
+            for (int k = 0; k < 5; ++k) {
+                I.un[k] = un + k * n;
+                I.ua[k] = ua + k * n;
+                I.ub[k] = ua + (5 + k) * n;
+            }
+            I.ratio[0] = ra;
+            I.ratio[1] = ra + n;
+            I.ldt = reinterpret_cast<double*>(take(n * sizeof(double)));
+            I.partial = reinterpret_cast<double*>(take(2 * (size_t)ntl * sizeof(double)));
+            double* far = reinterpret_cast<double*>(take(5 * (size_t)nj * sizeof(double)));
+            I.far = far;
+            I.res_hist = nullptr;
+            I.st = d_states_ + slot;
+            I.c = c;
+            cudaMemcpyAsync(d_xy, p.xy.data(), p.xy.size() * sizeof(double), cudaMemcpyHostToDevice, st_);
+            geometry_build(d_xy, p.n_rings, nj, g, st_);
+            JST_LAUNCH(k_far_geom, (nj + 255) / 256, 256, 0, st_, g, far);
+            JST_LAUNCH(k_fill_freestream, (unsigned)((n + 255) / 256), 256, 0, st_, I.un[0], I.un[1], I.un[2],
+                       I.un[3], I.un[4], (long)n, c);
+            InstState s0{};
+            s0.residual = std::numeric_limits<double>::quiet_NaN();
+            s0.target = p.raw.targetres;
+            s0.drop = p.drop;
+            s0.bad = fused::NO_BAD;
+            s0.fresh = 1;
+            s0.max_step = (int)std::min<int64_t>(p.max_steps, INT_MAX - 1);
+            h_states_[slot] = s0;
+            cudaMemcpyAsync(d_states_ + slot, &h_states_[slot], sizeof(InstState), cudaMemcpyHostToDevice, st_);
+            cudaMemcpyAsync(d_insts_ + slot, &h_insts_[slot], sizeof(Inst<T>), cudaMemcpyHostToDevice, st_);
+            int tile_off = (int)h_tiles_.size();
+            for (int a = 0; a < tiles_i; ++a)
+                for (int b = 0; b < tiles_j; ++b) h_tiles_.push_back(TileRef{slot, a * ti_, b * tj_, a * tiles_j + b});
+            counts_tmp_ = ntl;
+            cudaMemcpyAsync(d_counts_ + slot, &counts_tmp_, sizeof(int), cudaMemcpyHostToDevice, st_);
+            cudaMemcpyAsync(d_tiles_ + tile_off, h_tiles_.data() + tile_off, ntl * sizeof(TileRef),
+                            cudaMemcpyHostToDevice, st_);
+            JST_LAUNCH(K_.step_dt, ntl, K_.nt, 0, st_, d_tiles_ + tile_off, d_counts_ + slot, d_insts_, ti_, tj_);
+            cudaStreamSynchronize(st_);  // pageable sources above must stay valid until copied
+            ++active_;
+            queue_.pop_front();
+            changed = true;
+        }
+        if (changed) upload_tiles();
+        return cudaGetLastError() == cudaSuccess ? JST_OK : JST_ERR_CUDA;
+    }
+
+    void upload_tiles() {
+        ntiles_host_ = (int)h_tiles_.size();
+        if (ntiles_host_)
+            cudaMemcpyAsync(d_tiles_, h_tiles_.data(), h_tiles_.size() * sizeof(TileRef), cudaMemcpyHostToDevice,
+                            st_);
+        cudaMemcpyAsync(d_ntiles_, &ntiles_host_, sizeof(int), cudaMemcpyHostToDevice, st_);
+        cudaStreamSynchronize(st_);
+    }
+
+    void ensure_graph() {
+        if (graph_exec_) return;
+        int K = std::max(1, o_.steps_per_poll);
+        cudaGraph_t g;
+        cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal);
+        for (int q = 0; q < K; ++q)
+            for (int s = 0; s < 5; ++s) {
+                auto kern = s == 0 ? K_.stage[0] : (s == 4 ? K_.stage[2] : K_.stage[1]);
+                JST_LAUNCH(kern, grid_, K_.nt, K_.smem, st_, d_tiles_, d_ntiles_, d_insts_, s, RK_ALPHA[s]);
+            }
+        cudaStreamEndCapture(st_, &g);
+        cudaGraphInstantiate(&graph_exec_, g, 0);
+        cudaGraphDestroy(g);
+    }
+
+    void wall_force_launch(int slot) {
+        Slot& S = slots_[slot];
+        UnPtrs up;
+        for (int k = 0; k < 5; ++k) up.u[k] = h_insts_[slot].un[k];
+        launch_wall_force(S.g, up, h_insts_[slot].c, d_force_ + 2 * slot, st_);
+    }
+
+    void clcd_from(int slot, const double* f, double* cl, double* cd) {
+        Slot& S = slots_[slot];
+        const PhysConst& c = h_insts_[slot].c;
+        double q = 0.5 * c.rho_inf * (c.u_inf * c.u_inf + c.v_inf * c.v_inf) * S.chord;
+        *cd = (f[0] * std::cos(S.aoa) + f[1] * std::sin(S.aoa)) / q;
+        *cl = (-f[0] * std::sin(S.aoa) + f[1] * std::cos(S.aoa)) / q;
+    }
+
+    // Read every instance's device scalars, apply the CL window criterion,
+    // retire finished instances.
+    jst_status poll_retire() {
+        cudaMemcpyAsync(h_states_, d_states_, nslots_ * sizeof(InstState), cudaMemcpyDeviceToHost, st_);
+        if (cudaStreamSynchronize(st_) != cudaSuccess) return JST_ERR_CUDA;
+        std::vector<int> cl_slots;
+        for (int k = 0; k < nslots_; ++k)
+            if (slots_[k].used && slots_[k].cl_tol > 0.0 && h_states_[k].bad == fused::NO_BAD) {
+                const auto& h = slots_[k].cl_hist;
+                if (h.empty() || h_states_[k].step - h.back().first >= 50) cl_slots.push_back(k);
+            }
+        if (!cl_slots.empty()) {
+            for (int k : cl_slots) wall_force_launch(k);
+            std::vector<double> f(2 * nslots_);
+            cudaMemcpyAsync(f.data(), d_force_, f.size() * sizeof(double), cudaMemcpyDeviceToHost, st_);
+            cudaStreamSynchronize(st_);
+            for (int k : cl_slots) {
+                double cl, cd;
+                clcd_from(k, &f[2 * k], &cl, &cd);
+                slots_[k].cl_hist.emplace_back(h_states_[k].step, cl);
+            }
+        }
+        bool changed = false;
+        for (int k = 0; k < nslots_; ++k) {
+            Slot& S = slots_[k];
+            if (!S.used) continue;
+            const InstState& st = h_states_[k];
+            bool bad = st.bad != fused::NO_BAD;
+            bool cl_conv = false;
+            if (S.cl_tol > 0.0 && S.cl_hist.size() >= 2) {
+                const auto& h = S.cl_hist;
+                int cur = h.back().first;
+                for (size_t q = h.size() - 1; q-- > 0;)
+                    if (cur - h[q].first >= 100) {
+                        cl_conv = std::fabs(h.back().second - h[q].second) < S.cl_tol;
+                        break;
+                    }
+            }
+            if (!(bad || st.done || cl_conv || st.step >= S.max_steps)) continue;
+            retire(k, st, bad, st.done || cl_conv);
+            changed = true;
+        }
+        if (changed) {
+            std::vector<TileRef> keep;
+            keep.reserve(h_tiles_.size());
+            for (const TileRef& t : h_tiles_)
+                if (slots_[t.inst].used) keep.push_back(t);
+            h_tiles_.swap(keep);
+            upload_tiles();
+        }
+        return JST_OK;
+    }
+
+    void retire(int slot, const InstState& st, bool bad, bool converged) {
+        Slot& S = slots_[slot];
+        BatchResultFull R;
+        R.r.id = S.id;
+        R.r.steps = st.step;
+        R.r.residual = st.residual;
+        R.r.residual_first = st.res_first;
+        R.r.totaltime = st.totaltime;
+        R.r.t_submit = S.t_submit;
+        R.r.t_admit = S.t_admit;
+        R.r.ni = S.ni;
+        R.r.nj = S.nj;
+        R.r.status = bad ? JST_ERR_NONPHYSICAL : (converged ? JST_OK : JST_ERR_TIMEOUT);
+        if (bad) {
+            long id = (long)(st.bad & 0xffffffffULL);
+            int stage = (int)((st.bad >> 32) % 5);
+            double u[5];
+            for (int k = 0; k < 5; ++k) {
+                if (stage == 4) {
+                    cudaMemcpy(&u[k], h_insts_[slot].un[k] + id, sizeof(double), cudaMemcpyDeviceToHost);
+                } else {
+                    T v;
+                    cudaMemcpy(&v, (stage % 2 == 0 ? h_insts_[slot].ua[k] : h_insts_[slot].ub[k]) + id, sizeof(T),
+                               cudaMemcpyDeviceToHost);
+                    u[k] = (double)v;
+                }
+            }
+            nonphysical_report(h_insts_[slot].c, id / S.nj, id % S.nj, u, &R.r.bad);
+            R.r.cl = R.r.cd = std::numeric_limits<double>::quiet_NaN();
+        } else {
+            wall_force_launch(slot);
+            double f[2];
+            cudaMemcpyAsync(f, d_force_ + 2 * slot, sizeof f, cudaMemcpyDeviceToHost, st_);
+            cudaStreamSynchronize(st_);
+            clcd_from(slot, f, &R.r.cl, &R.r.cd);
+        }
+        if (o_.keep_fields) {
+            size_t n = (size_t)S.ni * S.nj;
+            R.fields.resize(5 * n);
+            for (int k = 0; k < 5; ++k)
+                cudaMemcpy(R.fields.data() + k * n, h_insts_[slot].un[k], n * sizeof(double), cudaMemcpyDeviceToHost);
+        }
+        R.r.t_done = now();
+        results_[S.id] = std::move(R);
+        finished_.push_back(S.id);
+        arena_.release(S.off, S.bytes);
+        S.used = false;
+        --active_;
+    }
+
+    jst_status step(int nsteps) override {
+        jst_status rc = admit();
+        if (rc != JST_OK) return rc;
+        ensure_graph();
+        int K = std::max(1, o_.steps_per_poll), done = 0;
+        while (done < nsteps && (active_ > 0 || !queue_.empty())) {
+            if (active_ == 0) {
+                admit();
+                if (active_ == 0) break;
+            }
+            cudaGraphLaunch(graph_exec_, st_);
+            done += K;
+            rc = poll_retire();
+            if (rc != JST_OK) return rc;
+            rc = admit();
+            if (rc != JST_OK) return rc;
+        }
+        return JST_OK;
+    }
+
+    void stats(int* a, int* q, double* bytes) override {
+        if (a) *a = active_;
+        if (q) *q = (int)queue_.size();
+        if (bytes) *bytes = (double)arena_.used;
+    }
+
+    int poll(int64_t* ids, int cap) override {
+        int n = 0;
+        while (!finished_.empty() && n < cap) {
+            ids[n++] = finished_.front();
+            finished_.pop_front();
+        }
+        return n;
+    }
+
+    bool result(int64_t id, BatchResultFull** out) override {
+        auto it = results_.find(id);
+        if (it == results_.end()) return false;
+        *out = &it->second;
+        return true;
+    }
+
+  private:
+    jst_batch_opts o_;
+    Clock::time_point t0_;
+    cudaStream_t st_ = nullptr;
+    Kernels<T> K_;
+    int ti_ = 8, tj_ = 32, grid_ = 1, nslots_ = 1, max_tiles_ = 0, ntiles_host_ = 0, counts_tmp_ = 0;
+    int active_ = 0;
+    int64_t next_id_ = 0;
+    void* small_ = nullptr;
+    Inst<T>* d_insts_ = nullptr;
+    InstState* d_states_ = nullptr;
+    InstState* h_states_ = nullptr;
+    double* d_force_ = nullptr;
+    int* d_counts_ = nullptr;
+    int* d_ntiles_ = nullptr;
+    TileRef* d_tiles_ = nullptr;
+    std::vector<Inst<T>> h_insts_;
+    std::vector<Slot> slots_;
+    std::vector<TileRef> h_tiles_;
+    std::deque<Pending> queue_;
+    std::map<int64_t, BatchResultFull> results_;
+    std::deque<int64_t> finished_;
+    Arena arena_;
+    cudaGraphExec_t graph_exec_ = nullptr;
+};
+
+}  // namespace jst
+
+struct jst_batch {
+    std::unique_ptr<jst::BatchBase> impl;
+};
+
+extern "C" {
+
+void jst_batch_default_opts(jst_batch_opts* o) {
+    std::memset(o, 0, sizeof *o);
+    o->precision = JST_PREC_FP32_SPLIT;
+    o->dt_mode = JST_DT_LOCAL;
+    o->max_instances = 256;
+    o->steps_per_poll = 20;
+    o->hbm_budget_gb = 0.0;
+}
+
+jst_status jst_batch_create(const jst_batch_opts* o, jst_batch** out) {
+    if (!o || !out) return JST_ERR_ARG;
+    std::string err;
+    std::unique_ptr<jst::BatchBase> impl;
+    if (o->precision == JST_PREC_FP64) {
+        auto* b = new jst::Batch<double>(*o);
+        impl.reset(b);
+        if (!b->create(err)) {
+            jst::set_call_error(err);
+            return JST_ERR_OOM;
+        }
+    } else {
+        auto* b = new jst::Batch<float>(*o);
+        impl.reset(b);
+        if (!b->create(err)) {
+            jst::set_call_error(err);
+            return JST_ERR_OOM;
+        }
+    }
+    *out = new jst_batch{std::move(impl)};
+    return JST_OK;
+}
+
+void jst_batch_destroy(jst_batch* b) { delete b; }
+
+jst_status jst_batch_submit(jst_batch* b, const char* cfg, const double* xy, int n_rings, int n_theta,
+                            int64_t max_steps, double residual_drop, double cl_tol, int64_t* id) {
+    if (!b || !cfg || !xy || !id) return JST_ERR_ARG;
+    return b->impl->submit(cfg, xy, n_rings, n_theta, max_steps, residual_drop, cl_tol, id);
+}
+
+jst_status jst_batch_step(jst_batch* b, int nsteps) { return b ? b->impl->step(nsteps) : JST_ERR_ARG; }
+
+jst_status jst_batch_stats(jst_batch* b, int* active, int* queued, double* bytes) {
+    if (!b) return JST_ERR_ARG;
+    b->impl->stats(active, queued, bytes);
+    return JST_OK;
+}
+
+jst_status jst_batch_poll(jst_batch* b, int64_t* ids, int cap, int* n) {
+    if (!b || !n || (cap > 0 && !ids)) return JST_ERR_ARG;
+    *n = b->impl->poll(ids, cap);
+    return JST_OK;
+}
+
+jst_status jst_batch_result_get(jst_batch* b, int64_t id, jst_batch_result* r, double* fields, size_t n) {
+    if (!b || !r) return JST_ERR_ARG;
+    jst::BatchResultFull* R = nullptr;
+    if (!b->impl->result(id, &R)) return JST_ERR_ARG;
+    *r = R->r;
+    if (fields) {
+        if (R->fields.empty() || n < R->fields.size()) return JST_ERR_ARG;
+        std::memcpy(fields, R->fields.data(), R->fields.size() * sizeof(double));
+    }
+    return JST_OK;
+}
+
+}  // extern "C"
+
+namespace jst {
 
 Engine* make_fused_engine(SolverCore* core, std::string& err) {
     if (core->opts.precision == JST_PREC_FP64) {

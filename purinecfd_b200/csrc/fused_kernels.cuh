@@ -35,6 +35,7 @@
 #ifndef JST_TID
 #define JST_TID() ((int)threadIdx.x)
 #define JST_BID() ((int)blockIdx.x)
+#define JST_GRID() (gridDim.x)
 #define JST_SYNC() __syncthreads()
 #define JST_FENCE() __threadfence()
 #endif
@@ -50,6 +51,8 @@ struct InstState {
     double totaltime;  // accumulated physical time (solver.rs:110-111)
     double residual;   // residual of the last completed step
     double target;     // solver.targetres
+    double drop;       // > 0: also stop when residual < drop * first residual
+    double res_first;  // residual of the first completed step
     unsigned long long bad;  // (stage_id << 32) | cell, NO_BAD when none
     unsigned int counter;    // last-block-done counter
     int step;          // completed steps
@@ -213,9 +216,10 @@ JST_D void finish_step(const Inst<T>& I, bool with_residual, double* red) {
             int step = st->step;
             st->residual = res;
             if (I.res_hist) I.res_hist[step] = res;
+            if (step == 0) st->res_first = res;
             st->step = step + 1;
             st->fresh = 0;
-            if (res < st->target) st->done = 1;
+            if (res < st->target || (st->drop > 0.0 && res < st->drop * st->res_first)) st->done = 1;
         }
         st->counter = 0;
     }
@@ -225,10 +229,13 @@ JST_D void finish_step(const Inst<T>& I, bool with_residual, double* red) {
 // plus the per-instance minimum: the time step of the first step and of any
 // step after the state was overwritten (timestep.rs:24-57).
 template <class T, int NT>
-__global__ void __launch_bounds__(NT) k_step_dt(const TileRef* tiles, const Inst<T>* insts, int TI, int TJ) {
+__global__ void __launch_bounds__(NT) k_step_dt(const TileRef* tiles, const int* ntiles, const Inst<T>* insts,
+                                                 int TI, int TJ) {
     __shared__ double red[NT];
     __shared__ int last;
-    TileRef tr = tiles[JST_BID()];
+    const int nt_all = *ntiles;
+    for (int tix = JST_BID(); tix < nt_all; tix += (int)JST_GRID()) {
+    TileRef tr = tiles[tix];
     const Inst<T>& I = insts[tr.inst];
     int fresh = I.st->fresh;
     double mloc = __longlong_as_double(0x7ff0000000000000LL);
@@ -266,6 +273,8 @@ __global__ void __launch_bounds__(NT) k_step_dt(const TileRef* tiles, const Inst
         JST_FENCE();
         finish_step<T, NT>(I, false, red);
     }
+    JST_SYNC();
+    }
 }
 
 // Asynchronous global -> shared copies (cp.async), one element each.
@@ -287,7 +296,8 @@ JST_D void async_wait_all() {
 // The stage kernel.  FIRST: stage 0 (reads U_n, adds dt to the total time).
 // LAST: stage 4 (writes U_n in place, residual, next step's time step).
 template <class T, int TI, int TJ, int NT, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T>* insts, int stage, double alpha) {
+__global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* ntiles, const Inst<T>* insts, int stage,
+                                              double alpha) {
     using L = Layout<T, TI, TJ, NT>;
     using TS = typename std::conditional<FIRST, double, T>::type;
     using TD = typename std::conditional<LAST, double, T>::type;
@@ -299,8 +309,10 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
     double* red = reinterpret_cast<double*>(smem_raw + L::red_off);
     double* farbuf = red + NT;  // 7 values per staged column of a far-field tile
     __shared__ int flags[4];
-
-    const TileRef tr = tiles[JST_BID()];
+    const int nt_all = *ntiles;
+    // Persistent over the tile table: blocks stride through (instance, tile) items.
+    for (int tix = JST_BID(); tix < nt_all; tix += (int)JST_GRID()) {
+    const TileRef tr = tiles[tix];
     const Inst<T>& I = insts[tr.inst];
     const int ni = I.ni, nj = I.nj, i0 = tr.i0, j0 = tr.j0;
     const PhysConst& c = I.c;
@@ -318,7 +330,10 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
         if (FIRST && !skip && tr.tile == 0) st->totaltime += st->dt;
     }
     JST_SYNC();
-    if (flags[0]) return;
+    if (flags[0]) {
+        JST_SYNC();  // flags is rewritten by the next item
+        continue;
+    }
     const int fresh = flags[1];
     const unsigned long long stage_id = (unsigned long long)flags[2] * 5 + stage;
     const T* ratio = I.ratio[flags[2] & 1];
@@ -718,6 +733,8 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const Inst<T
             JST_FENCE();
             finish_step<T, NT>(I, true, red);
         }
+    }
+    JST_SYNC();  // shared memory is reused by the next item
     }
 }
 
