@@ -212,10 +212,13 @@ def run_ours(args, world, rank, local):
     cfg, xy, nr, nt = workloads.WORKLOADS[args.workload]()
     tile = {}
     if args.tile:
-        ti, tj = (int(x) for x in args.tile.lower().split("x"))
-        tile = {"tile_i": ti, "tile_j": tj}
+        parts = [int(x) for x in args.tile.lower().split("x")]
+        tile = {"tile_i": parts[0], "tile_j": parts[1]}
+        if len(parts) > 2:
+            tile["block_threads"] = parts[2]
     s = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=local, **tile)
     cells = s.n_cells
+    kcfg = s.kernel_config()
     s.time_steps(args.warmup)
     barrier(world)
     with ClockSampler(local) as clk:
@@ -233,7 +236,7 @@ def run_ours(args, world, rank, local):
             "dtype": "f32+f64" if args.precision == "split" else "f64", "data": "synthetic",
             "config": {"workload": args.workload, "cells": cells, "precision": args.precision,
                        "path": "fused tiled stage kernel, CUDA graph per RK step",
-                       "tile": args.tile or "default",
+                       "tile": "x".join(map(str, kcfg)) + (" (autotuned)" if not args.tile else ""),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (state + geometry ~0.7 GB)"},
             "gpu_launches": 5 * args.steps, "residual_after": residual}

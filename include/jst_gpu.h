@@ -72,6 +72,7 @@ typedef struct {
     int tile_j;      /* fused path tile columns (0 = autotuned) */
     int use_graph;   /* capture each RK step as a CUDA graph (fused path) */
     double nut_inf_ratio; /* free-stream nu-tilde / nu; <= 0 uses the config value or 0.1 */
+    int block_threads;    /* fused path threads per block (0 = default for the tile) */
 } jst_opts;
 
 /* Fills opts with the defaults: FP64, global dt, fused path, device 0,
@@ -212,6 +213,7 @@ typedef struct {
     int steps_per_poll;   /* RK steps per graph replay between convergence polls */
     double hbm_budget_gb; /* device memory the batch may hold for instances */
     int keep_fields;      /* copy U of retired instances to host memory */
+    int block_threads;    /* threads per block (0 = default for the tile) */
 } jst_batch_opts;
 
 void jst_batch_default_opts(jst_batch_opts* o);
@@ -268,6 +270,10 @@ jst_status jst_batch_result_get(jst_batch* b, int64_t id, jst_batch_result* r, d
  * on the GPU race, so serialise them (one stream, or events). */
 jst_status jst_residual_noalloc(const double* rho, const double* rho_prev, int ni, int nj, double* out,
                                 void* stream);
+
+/* Tile shape and block size the fused path runs with (chosen by the
+ * autotuner when jst_opts.tile_i/tile_j are 0); zeros on the passes path. */
+jst_status jst_kernel_config(const jst_solver* s, int* tile_i, int* tile_j, int* block_threads);
 
 /* Version string of this library. */
 const char* jst_version(void);

@@ -20,7 +20,7 @@ from .solver import (DT_LOCAL, OK, PREC_FP32_SPLIT, JstError, NonPhysicalC, lib)
 class BatchOptsC(C.Structure):
     _fields_ = [("precision", C.c_int), ("dt_mode", C.c_int), ("device", C.c_int), ("tile_i", C.c_int),
                 ("tile_j", C.c_int), ("max_instances", C.c_int), ("steps_per_poll", C.c_int),
-                ("hbm_budget_gb", C.c_double), ("keep_fields", C.c_int)]
+                ("hbm_budget_gb", C.c_double), ("keep_fields", C.c_int), ("block_threads", C.c_int)]
 
 
 class BatchResultC(C.Structure):
@@ -72,13 +72,14 @@ def _bind():
 
 class Batch:
     def __init__(self, precision=PREC_FP32_SPLIT, dt_mode=DT_LOCAL, device=0, tile_i=0, tile_j=0,
-                 max_instances=256, steps_per_poll=20, hbm_budget_gb=0.0, keep_fields=False):
+                 max_instances=256, steps_per_poll=20, hbm_budget_gb=0.0, keep_fields=False, block_threads=0):
         L = _bind()
         o = BatchOptsC()
         L.jst_batch_default_opts(C.byref(o))
         o.precision, o.dt_mode, o.device, o.tile_i, o.tile_j = precision, dt_mode, device, tile_i, tile_j
         o.max_instances, o.steps_per_poll, o.hbm_budget_gb = max_instances, steps_per_poll, hbm_budget_gb
         o.keep_fields = 1 if keep_fields else 0
+        o.block_threads = block_threads
         h = C.c_void_p()
         rc = L.jst_batch_create(C.byref(o), C.byref(h))
         if rc != OK:

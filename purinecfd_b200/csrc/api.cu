@@ -606,6 +606,12 @@ jst_status jst_write_csv(jst_solver* s, const char* path) {
     return JST_OK;
 }
 
+jst_status jst_kernel_config(const jst_solver* s, int* ti, int* tj, int* nt) {
+    if (!s || !ti || !tj || !nt) return JST_ERR_ARG;
+    s->eng->kernel_config(ti, tj, nt);
+    return JST_OK;
+}
+
 jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_ms) {
     if (!s || !ms || nsteps < 0) return JST_ERR_ARG;
     int64_t before = 0;

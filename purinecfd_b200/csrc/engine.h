@@ -68,6 +68,11 @@ class Engine {
         return rc;
     }
     virtual cudaStream_t stream() const = 0;
+    virtual void kernel_config(int* ti, int* tj, int* nt) const {
+        *ti = 0;
+        *tj = 0;
+        *nt = 0;
+    }
     virtual void set_uniform(double, double, double, double, double) {}
     virtual void run_kernel(const char*) {}
 

@@ -17,6 +17,8 @@
 #include <chrono>
 #include <deque>
 #include <map>
+#include <mutex>
+#include <tuple>
 
 #include "config_mesh.h"
 #include "engine.h"
@@ -141,7 +143,7 @@ void launch_wall_force(const Geom& g, const UnPtrs& up, const PhysConst& c, doub
 }
 
 // Tile configurations compiled into the library: (TI, TJ, NT).
-#define JST_FOR_TILES(X) X(4, 32, 256) X(8, 32, 256) X(16, 32, 256) X(4, 64, 256) X(8, 64, 256)
+#define JST_FOR_TILES(X) X(4, 32, 256) X(8, 32, 256) X(16, 32, 256) X(4, 64, 256) X(8, 64, 256) X(8, 32, 192) X(8, 32, 128) X(16, 32, 384)
 
 template <class T> struct Kernels {
     void (*stage[3])(const TileRef*, const int*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};
@@ -161,11 +163,11 @@ template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
     return k;
 }
 
-template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out) {
-#define JST_PICK(a, b, n)                    \
-    if (ti == a && tj == b) {                \
-        *out = kernels_for<T, a, b, n>();    \
-        return true;                         \
+template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 256) {
+#define JST_PICK(a, b, n)                               \
+    if (ti == a && tj == b && nt == n) {                \
+        *out = kernels_for<T, a, b, n>();               \
+        return true;                                    \
     }
     JST_FOR_TILES(JST_PICK)
 #undef JST_PICK
@@ -183,6 +185,97 @@ void default_tile(int prec, int nj, int* ti, int* tj) {
     }
 }
 
+// Tile configurations the autotuner times, in order (TI, TJ, threads).
+const int kTileCands[][3] = {{8, 32, 256}, {8, 32, 192}, {16, 32, 384}, {16, 32, 256}, {4, 32, 256},
+                             {4, 64, 256},  {8, 64, 256}, {8, 32, 128}};
+
+// Stage input buffer = T copy of U_n, so a middle stage can be timed without
+// touching the solution.
+template <class T> __global__ void k_copy_state(Inst<T> I, long n) {
+    long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    for (int k = 0; k < 5; ++k) I.ua[k][id] = (T)I.un[k][id];
+}
+
+struct TuneResult {
+    int ti, tj, nt;
+    float ms;
+};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, TuneResult> g_tune_cache;
+
+std::vector<TileRef> make_tiles(int inst, int ni, int nj, int ti, int tj) {
+    std::vector<TileRef> t;
+    int a_n = (ni + ti - 1) / ti, b_n = (nj + tj - 1) / tj;
+    t.reserve((size_t)a_n * b_n);
+    for (int a = 0; a < a_n; ++a)
+        for (int b = 0; b < b_n; ++b) t.push_back(TileRef{inst, a * ti, b * tj, a * b_n + b});
+    return t;
+}
+
+// Times one middle-stage launch per candidate over the given instances
+// (their U_a must hold a valid state) and returns the fastest configuration.
+template <class T>
+TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& insts, Inst<T>* d_insts,
+                    InstState* d_states, int nstates, cudaStream_t st, int grid_hint) {
+    TuneResult best{8, 32, 256, 1e30f};
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    TileRef* d_t = nullptr;
+    int* d_n = nullptr;
+    size_t cap = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (const auto& cand : kTileCands) {
+        Kernels<T> K;
+        if (!pick_kernels<T>(cand[0], cand[1], &K, cand[2])) continue;
+        if (cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        std::vector<TileRef> tiles;
+        for (const auto& in : insts) {
+            auto t = make_tiles(in.first, in.second.first, in.second.second, cand[0], cand[1]);
+            tiles.insert(tiles.end(), t.begin(), t.end());
+        }
+        if (tiles.size() > cap) {
+            if (d_t) cudaFree(d_t);
+            cap = tiles.size();
+            cudaMalloc(&d_t, cap * sizeof(TileRef) + 256);
+            if (!d_n) cudaMalloc(&d_n, sizeof(int));
+        }
+        int nt_ = (int)tiles.size();
+        cudaMemcpyAsync(d_t, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_n, &nt_, sizeof(int), cudaMemcpyHostToDevice, st);
+        int occ = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K.stage[1], K.nt, K.smem);
+        int grid = grid_hint > 0 ? std::min(nt_, sms * std::max(1, occ)) : nt_;
+        JST_LAUNCH(K.stage[1], grid, K.nt, K.smem, st, d_t, d_n, d_insts, 1, RK_ALPHA[1]);  // warm-up
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3; ++r) JST_LAUNCH(K.stage[1], grid, K.nt, K.smem, st, d_t, d_n, d_insts, 1, RK_ALPHA[1]);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best.ms) best = TuneResult{cand[0], cand[1], cand[2], ms};
+    }
+    // undo any NonPhysical flag the timing launches may have raised
+    std::vector<InstState> hs(nstates);
+    cudaMemcpy(hs.data(), d_states, nstates * sizeof(InstState), cudaMemcpyDeviceToHost);
+    for (auto& x : hs) x.bad = fused::NO_BAD;
+    cudaMemcpy(d_states, hs.data(), nstates * sizeof(InstState), cudaMemcpyHostToDevice);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (d_t) cudaFree(d_t);
+    if (d_n) cudaFree(d_n);
+    return best;
+}
+
 }  // namespace
 
 template <class T> class FusedEngine : public Engine {
@@ -194,29 +287,38 @@ template <class T> class FusedEngine : public Engine {
         if (h_state_) cudaFreeHost(h_state_);
     }
 
-    bool create(std::string& err) {
-        SolverCore& C = *core_;
-        int ti = C.opts.tile_i, tj = C.opts.tile_j;
-        if (ti <= 0 || tj <= 0) default_tile(C.opts.precision, C.nj, &ti, &tj);
-        if (!pick_kernels<T>(ti, tj, &K_)) {
-            err = "unsupported tile shape " + std::to_string(ti) + "x" + std::to_string(tj);
+    bool select_kernels(int ti, int tj, int nt, std::string& err) {
+        if (!pick_kernels<T>(ti, tj, &K_, nt)) {
+            err = "unsupported tile shape " + std::to_string(ti) + "x" + std::to_string(tj) + "x" + std::to_string(nt);
             return false;
         }
-        ti_ = ti;
-        tj_ = tj;
         for (int k = 0; k < 3; ++k)
             if (cudaFuncSetAttribute(K_.stage[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K_.smem) !=
                 cudaSuccess) {
                 err = "stage kernel needs " + std::to_string(K_.smem) + " bytes of shared memory";
                 return false;
             }
+        ti_ = ti;
+        tj_ = tj;
+        return true;
+    }
+
+    bool create(std::string& err) {
+        SolverCore& C = *core_;
+        int ti = C.opts.tile_i, tj = C.opts.tile_j, nt = C.opts.block_threads > 0 ? C.opts.block_threads : 256;
+        tune_ = ti <= 0 || tj <= 0;
+        if (tune_) {
+            default_tile(C.opts.precision, C.nj, &ti, &tj);
+            nt = 256;
+        }
+        if (!select_kernels(ti, tj, nt, err)) return false;
         int ni = C.ni, nj = C.nj;
-        int tiles_i = (ni + ti - 1) / ti, tiles_j = (nj + tj - 1) / tj;
-        ntiles_ = tiles_i * tiles_j;
-        std::vector<TileRef> tiles;
-        tiles.reserve(ntiles_);
-        for (int a = 0; a < tiles_i; ++a)
-            for (int b = 0; b < tiles_j; ++b) tiles.push_back(TileRef{0, a * ti, b * tj, a * tiles_j + b});
+        std::vector<TileRef> tiles = make_tiles(0, ni, nj, ti, tj);
+        ntiles_ = (int)tiles.size();
+        int max_tiles = ntiles_;  // the autotuner may pick a smaller tile
+        if (tune_)
+            for (const auto& cd : kTileCands)
+                max_tiles = std::max(max_tiles, ((ni + cd[0] - 1) / cd[0]) * ((nj + cd[1] - 1) / cd[1]));
         size_t n = (size_t)ni * nj;
         size_t bytes = 0;
         auto add = [&](size_t b) {
@@ -227,13 +329,14 @@ template <class T> class FusedEngine : public Engine {
         size_t o_un = add(5 * n * sizeof(double));
         size_t o_ua = add(5 * n * sizeof(T));
         size_t o_ub = add(5 * n * sizeof(T));
+        size_t o_uc = add(sizeof(T) == sizeof(double) ? 0 : 5 * n * sizeof(T));
         size_t o_ratio = add(2 * n * sizeof(T));
         size_t o_ldt = add(n * sizeof(double));
-        size_t o_partial = add(2 * (size_t)ntiles_ * sizeof(double));
+        size_t o_partial = add(2 * (size_t)max_tiles * sizeof(double));
         size_t o_far = add(5 * (size_t)nj * sizeof(double));
         size_t o_st = add(sizeof(InstState));
         size_t o_inst = add(sizeof(Inst<T>));
-        size_t o_tiles = add(tiles.size() * sizeof(TileRef));
+        size_t o_tiles = add((size_t)max_tiles * sizeof(TileRef));
         size_t o_force = add(8 * sizeof(double));
         size_t o_ntiles = add(sizeof(int));
         size_t o_unptr = add(5 * sizeof(double*));
@@ -262,6 +365,7 @@ template <class T> class FusedEngine : public Engine {
             I.un[k] = reinterpret_cast<double*>(base + o_un) + k * n;
             I.ua[k] = reinterpret_cast<T*>(base + o_ua) + k * n;
             I.ub[k] = reinterpret_cast<T*>(base + o_ub) + k * n;
+            I.uc[k] = sizeof(T) == sizeof(double) ? nullptr : reinterpret_cast<T*>(base + o_uc) + k * n;
         }
         I.ratio[0] = reinterpret_cast<T*>(base + o_ratio);
         I.ratio[1] = I.ratio[0] + n;
@@ -313,6 +417,50 @@ template <class T> class FusedEngine : public Engine {
                    inst_.un[2], inst_.un[3], inst_.un[4], n, C.c);
         reset_state(1);
         launch_step_dt();
+        if (tune_) tune();
+    }
+
+    // Autotuner: time every compiled tile configuration on this mesh (one
+    // middle-stage launch on a copy of the state each) and keep the fastest;
+    // the choice is cached per (precision, NI, NJ, time-step mode).
+    void tune() {
+        SolverCore& C = *core_;
+        auto key = std::make_tuple((int)sizeof(T), C.ni, C.nj, C.local_dt);
+        TuneResult r{};
+        bool have = false;
+        {
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            auto it = g_tune_cache.find(key);
+            if (it != g_tune_cache.end()) {
+                r = it->second;
+                have = true;
+            }
+        }
+        if (!have) {
+            long n = (long)C.ni * C.nj;
+            JST_LAUNCH(k_copy_state<T>, (unsigned)((n + 255) / 256), 256, 0, C.st, inst_, n);
+            r = autotune<T>({{0, {C.ni, C.nj}}}, d_inst_, inst_.st, 1, C.st, 0);
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            g_tune_cache[key] = r;
+        }
+        std::string err;
+        if (!select_kernels(r.ti, r.tj, r.nt, err)) return;
+        std::vector<TileRef> tiles = make_tiles(0, C.ni, C.nj, r.ti, r.tj);
+        ntiles_ = (int)tiles.size();
+        inst_.ntiles = ntiles_;
+        cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
+        cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, C.st);
+        cudaMemcpyAsync(d_ntiles_, &ntiles_, sizeof(int), cudaMemcpyHostToDevice, C.st);
+        reset_state(1);
+        launch_step_dt();
+        cudaStreamSynchronize(C.st);
+    }
+
+  public:
+    void kernel_config(int* ti, int* tj, int* nt) const override {
+        *ti = ti_;
+        *tj = tj_;
+        *nt = K_.nt;
     }
 
     void launch_step_dt() {
@@ -609,6 +757,7 @@ template <class T> class FusedEngine : public Engine {
     SolverCore* core_;
     Kernels<T> K_;
     int ti_ = 8, tj_ = 32, ntiles_ = 0;
+    bool tune_ = false;
     void* arena_ = nullptr;
     double* extra_hist_ = nullptr;
     size_t hist_cap_ = 0;
@@ -734,24 +883,16 @@ template <class T> class Batch : public BatchBase {
             return false;
         }
         cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
-        int ti = o_.tile_i, tj = o_.tile_j;
-        if (ti <= 0 || tj <= 0) default_tile(o_.precision, 128, &ti, &tj);
-        if (!pick_kernels<T>(ti, tj, &K_)) {
+        int ti = o_.tile_i, tj = o_.tile_j, nt = o_.block_threads > 0 ? o_.block_threads : 256;
+        tune_ = ti <= 0 || tj <= 0;
+        if (tune_) {
+            default_tile(o_.precision, 128, &ti, &tj);
+            nt = 256;
+        }
+        if (!select_kernels(ti, tj, nt)) {
             err = "unsupported tile shape";
             return false;
         }
-        ti_ = ti;
-        tj_ = tj;
-        for (int k = 0; k < 3; ++k)
-            if (cudaFuncSetAttribute(K_.stage[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K_.smem) !=
-                cudaSuccess) {
-                err = "stage kernel shared memory too large";
-                return false;
-            }
-        int sms = 0, occ = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o_.device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K_.stage[1], K_.nt, K_.smem);
-        grid_ = std::max(1, sms * std::max(1, occ));
         nslots_ = std::max(1, o_.max_instances);
         max_tiles_ = 1 << 22;
         size_t bytes = nslots_ * (sizeof(Inst<T>) + sizeof(InstState) + sizeof(int) + 2 * sizeof(double)) +
@@ -793,6 +934,58 @@ template <class T> class Batch : public BatchBase {
         int zero = 0;
         cudaMemcpy(d_ntiles_, &zero, sizeof zero, cudaMemcpyHostToDevice);
         return true;
+    }
+
+    bool select_kernels(int ti, int tj, int nt) {
+        Kernels<T> K;
+        if (!pick_kernels<T>(ti, tj, &K, nt)) return false;
+        for (int k = 0; k < 3; ++k)
+            if (cudaFuncSetAttribute(K.stage[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) !=
+                cudaSuccess)
+                return false;
+        K_ = K;
+        ti_ = ti;
+        tj_ = tj;
+        int sms = 0, occ = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o_.device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K_.stage[1], K_.nt, K_.smem);
+        grid_ = std::max(1, sms * std::max(1, occ));
+        return true;
+    }
+
+    // Autotuner over the instances admitted so far (before the graph is
+    // captured): every candidate tile configuration times one middle-stage
+    // launch over the whole batch; the fastest is kept and all instances are
+    // re-tiled with it.
+    void tune() {
+        tune_ = false;
+        std::vector<std::pair<int, std::pair<int, int>>> list;
+        for (int k = 0; k < nslots_; ++k)
+            if (slots_[k].used) {
+                list.push_back({k, {slots_[k].ni, slots_[k].nj}});
+                long n = (long)slots_[k].ni * slots_[k].nj;
+                JST_LAUNCH(k_copy_state<T>, (unsigned)((n + 255) / 256), 256, 0, st_, h_insts_[k], n);
+            }
+        if (list.empty()) return;
+        TuneResult r = autotune<T>(list, d_insts_, d_states_, nslots_, st_, 1);
+        if (!select_kernels(r.ti, r.tj, r.nt)) return;
+        h_tiles_.clear();
+        for (int k = 0; k < nslots_; ++k)
+            if (slots_[k].used) {
+                auto t = make_tiles(k, slots_[k].ni, slots_[k].nj, ti_, tj_);
+                slots_[k].ntiles = (int)t.size();
+                h_insts_[k].ntiles = (int)t.size();
+                cudaMemcpyAsync(d_insts_ + k, &h_insts_[k], sizeof(Inst<T>), cudaMemcpyHostToDevice, st_);
+                h_tiles_.insert(h_tiles_.end(), t.begin(), t.end());
+            }
+        upload_tiles();
+    }
+
+    int max_tiles_for(int ni, int nj) const {
+        int m = ((ni + ti_ - 1) / ti_) * ((nj + tj_ - 1) / tj_);
+        if (tune_)
+            for (const auto& cd : kTileCands) m = std::max(m, ((ni + cd[0] - 1) / cd[0]) * ((nj + cd[1] - 1) / cd[1]));
+        return m;
     }
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0_).count(); }
@@ -845,7 +1038,7 @@ template <class T> class Batch : public BatchBase {
         add((10 * n + 4 * ntau) * sizeof(double));  // geometry
         add(2 * (size_t)nr * nt * sizeof(double));  // nodes
         add(5 * n * sizeof(double));                 // U_n
-        add(10 * n * sizeof(T));                     // U_a, U_b
+        add((sizeof(T) == sizeof(double) ? 10 : 15) * n * sizeof(T));  // U_a, U_b (+ U_c)
         add(2 * n * sizeof(T));                      // ratio
         add(n * sizeof(double));                     // localdt
         add(2 * (size_t)ntiles * sizeof(double));    // partials
@@ -868,7 +1061,8 @@ template <class T> class Batch : public BatchBase {
             int ni = p.n_rings - 1, nj = p.n_theta;
             int tiles_i = (ni + ti_ - 1) / ti_, tiles_j = (nj + tj_ - 1) / tj_, ntl = tiles_i * tiles_j;
             if ((long)h_tiles_.size() + ntl > max_tiles_) break;
-            size_t bytes = instance_bytes(p.n_rings, p.n_theta, ntl), off = 0;
+            int ptl = max_tiles_for(ni, nj);
+            size_t bytes = instance_bytes(p.n_rings, p.n_theta, ptl), off = 0;
             if (!arena_.alloc(bytes, &off)) break;
             Slot& S = slots_[slot];
             S = Slot{};
@@ -933,17 +1127,18 @@ template <class T> class Batch : public BatchBase {
             I.inv_vol = g.inv_vol;
             I.inv_d2 = g.inv_d2;
             double* un = reinterpret_cast<double*>(take(5 * n * sizeof(double)));
-            T* ua = reinterpret_cast<T*>(take(10 * n * sizeof(T)));
+            T* ua = reinterpret_cast<T*>(take((sizeof(T) == sizeof(double) ? 10 : 15) * n * sizeof(T)));
             T* ra = reinterpret_cast<T*>(take(2 * n * sizeof(T)));
             for (int k = 0; k < 5; ++k) {
                 I.un[k] = un + k * n;
                 I.ua[k] = ua + k * n;
                 I.ub[k] = ua + (5 + k) * n;
+                I.uc[k] = sizeof(T) == sizeof(double) ? nullptr : ua + (10 + k) * n;
             }
             I.ratio[0] = ra;
             I.ratio[1] = ra + n;
             I.ldt = reinterpret_cast<double*>(take(n * sizeof(double)));
-            I.partial = reinterpret_cast<double*>(take(2 * (size_t)ntl * sizeof(double)));
+            I.partial = reinterpret_cast<double*>(take(2 * (size_t)ptl * sizeof(double)));
             double* far = reinterpret_cast<double*>(take(5 * (size_t)nj * sizeof(double)));
             I.far = far;
             I.res_hist = nullptr;
@@ -1126,6 +1321,7 @@ template <class T> class Batch : public BatchBase {
     jst_status step(int nsteps) override {
         jst_status rc = admit();
         if (rc != JST_OK) return rc;
+        if (tune_ && active_ > 0) tune();
         ensure_graph();
         int K = std::max(1, o_.steps_per_poll), done = 0;
         while (done < nsteps && (active_ > 0 || !queue_.empty())) {
@@ -1172,6 +1368,7 @@ template <class T> class Batch : public BatchBase {
     Kernels<T> K_;
     int ti_ = 8, tj_ = 32, grid_ = 1, nslots_ = 1, max_tiles_ = 0, ntiles_host_ = 0, counts_tmp_ = 0;
     int active_ = 0;
+    bool tune_ = false;
     int64_t next_id_ = 0;
     void* small_ = nullptr;
     Inst<T>* d_insts_ = nullptr;

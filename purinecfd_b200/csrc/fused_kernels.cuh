@@ -29,6 +29,10 @@
 
 #include "jst_common.cuh"
 
+#ifndef JST_PREFETCH_UN
+#define JST_PREFETCH_UN 0  // stage the tile's U_n in shared memory with the geometry
+#endif
+
 #ifndef JST_DYN_SMEM
 #define JST_DYN_SMEM(name) extern __shared__ __align__(16) unsigned char name[]
 #endif
@@ -74,6 +78,7 @@ template <class T> struct Inst {
     double* un[5];      // U_n, the FP64 step-start state
     T* ua[5];           // stage ping-pong buffers
     T* ub[5];
+    T* uc[5];           // split mode: T copy of U_n written by the last stage, staged by stage 0
     T* ratio[2];        // V / localdt, indexed by step parity (dissipation.rs:51-56)
     double* ldt;        // localdt of the current step (local time stepping)
     double* partial;    // per tile: min localdt, sum (drho)^2
@@ -111,7 +116,7 @@ template <class T, int TI, int TJ, int NT> struct Layout {
     // FP64 geometry block: tau nx, ny; n nx, ny; 1/V on tile + ring; V and 1/d^2 on the tile
     static constexpr size_t goff = ((size_t)tsize * sizeof(T) + 15) / 16 * 16;
     static constexpr int gTx = 0, gTy = NGT, gNx = 2 * NGT, gNy = 2 * NGT + NGN, gIV = 2 * NGT + 2 * NGN,
-                         gV = gIV + NR, gD2 = gV + TT, gUn = gD2 + TT, gsize = gUn + 5 * TT;
+                         gV = gIV + NR, gD2 = gV + TT, gUn = gD2 + TT, gsize = gUn + (JST_PREFETCH_UN ? 5 * TT : 0);
     static constexpr size_t red_off = goff + (size_t)gsize * sizeof(double);
     static constexpr size_t bytes = red_off + (size_t)(NT + 7 * LJ) * sizeof(double);
 };
@@ -255,6 +260,8 @@ __global__ void __launch_bounds__(NT) k_step_dt(const TileRef* tiles, const int*
             v = q.vy;
             t = q.t;
         }
+        if (sizeof(T) != sizeof(double))
+            for (int k = 0; k < 5; ++k) I.uc[k][id] = (T)I.un[k][id];
         double dl = cell_localdt<T>(I, i, j, u, v, t);
         I.ratio[I.st->step & 1][id] = (T)(ld(I.vol + id) / dl);
         if (I.local_dt) I.ldt[id] = dl;
@@ -299,9 +306,11 @@ template <class T, int TI, int TJ, int NT, bool FIRST, bool LAST>
 __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* ntiles, const Inst<T>* insts, int stage,
                                               double alpha) {
     using L = Layout<T, TI, TJ, NT>;
-    using TS = typename std::conditional<FIRST, double, T>::type;
+    // Stage 0 reads U_n; in the split mode it stages the T copy of U_n that the
+    // previous last stage wrote, so every stage stages T values asynchronously.
+    using TS = T;
     using TD = typename std::conditional<LAST, double, T>::type;
-    constexpr bool ASYNC_U = std::is_same<TS, T>::value;
+    constexpr bool ASYNC_U = true;
     constexpr int LJ = L::LJ, NL = L::NL, RJ = L::RJ, NR = L::NR, TT = L::TT;
     JST_DYN_SMEM(smem_raw);
     T* sm = reinterpret_cast<T*>(smem_raw);
@@ -343,7 +352,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
     const TS* src[5];
     TD* dst[5];
     for (int k = 0; k < 5; ++k) {
-        if (FIRST) src[k] = reinterpret_cast<const TS*>(I.un[k]);
+        if (FIRST) src[k] = sizeof(T) == sizeof(double) ? reinterpret_cast<const TS*>(I.un[k]) : I.uc[k];
         else src[k] = reinterpret_cast<const TS*>((stage % 2 == 1) ? I.ua[k] : I.ub[k]);
         if (LAST) dst[k] = reinterpret_cast<TD*>(I.un[k]);
         else dst[k] = reinterpret_cast<TD*>((stage % 2 == 0) ? I.ua[k] : I.ub[k]);
@@ -402,12 +411,14 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
             gs[L::gD2 + e] = 0.0;
         }
     }
+#if JST_PREFETCH_UN
     for (int e = tid; e < TT; e += NT) {  // U_n of the tile cells, for the update
         int r = e / TJ, cc = e - r * TJ;
         int gi = i0 + r, gj = j0 + cc;
         if (gi < ni && gj < nj)
             for (int k = 0; k < 5; ++k) async_copy<8>(gs + L::gUn + k * TT + e, I.un[k] + (long)gi * nj + gj);
     }
+#endif
     constexpr int KA = (NL + NT - 1) / NT;
     TS rawr[ASYNC_U ? 1 : KA][5];
 #pragma unroll
@@ -663,7 +674,11 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
         if (gi >= ni || gj >= nj) continue;
         long id = (long)gi * nj + gj;
         double uo[5];
+#if JST_PREFETCH_UN
         for (int k = 0; k < 5; ++k) uo[k] = gs[L::gUn + k * TT + w];
+#else
+        for (int k = 0; k < 5; ++k) uo[k] = I.un[k][id];
+#endif
         T R[5];
         const int fd = ti * (TJ + 1) + tj;
         for (int k = 0; k < 5; ++k)
@@ -677,11 +692,12 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
             if (sizeof(T) == sizeof(double)) un[k] = uo[k] - (double)R[k] * sc;
             else un[k] = uo[k] - (double)(R[k] * (T)sc);  // FP32 increment, FP64 accumulator
             dst[k][id] = (TD)un[k];
+            if (LAST && sizeof(T) != sizeof(double)) I.uc[k][id] = (T)un[k];
         }
         // unpack checks (solver.rs:160-171), on the stored precision
         bool bad;
         Prim<double> q{};
-        if (LAST || sizeof(T) == sizeof(double)) {
+        if (sizeof(T) == sizeof(double)) {
             double rho = un[0];
             bad = isnan(rho) || rho <= 1e-15;
             if (!bad) {
@@ -692,9 +708,11 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
             T rho = (T)un[0];
             bad = isnan(rho) || rho <= T(1e-15);
             if (!bad) {
-                T inv = T(1) / rho, vx = (T)un[1] * inv, vy = (T)un[2] * inv;
-                T p = (T)c.gm1 * ((T)un[3] - rho * (vx * vx + vy * vy) * T(0.5));
-                bad = isnan(p) || p <= T(1e-15);
+                Prim<T> qt = unpack_cell<T>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], (T)c.gm1, (T)c.r_gas);
+                bad = isnan(qt.p) || qt.p <= T(1e-15);
+                q.vx = qt.vx;
+                q.vy = qt.vy;
+                q.t = qt.t;
             }
         }
         if (bad) {
@@ -704,18 +722,19 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
         if (LAST) {
             double d = un[0] - uo[0];  // solver.rs:195
             sres += d * d;
-            // timestep.rs:30-42 from the staged geometry
+            // timestep.rs:30-42 from the staged geometry, in the stage arithmetic
             int tdn = (ti + 1) * L::GTJ + tj + 1, tup = tdn + L::GTJ;
             int nlf = (ti + 1) * L::GNJ + tj + 1, nrt = nlf + 1;
-            double aa = 0.5 * (gs[L::gTx + tdn] + gs[L::gTx + tup]);
-            double bb = 0.5 * (gs[L::gTy + tdn] + gs[L::gTy + tup]);
-            double cc = 0.5 * (gs[L::gNx + nlf] + gs[L::gNx + nrt]);
-            double dd = 0.5 * (gs[L::gNy + nlf] + gs[L::gNy + nrt]);
-            double vol = gs[L::gV + w];
-            double dl = local_dt<double>(q.vx, q.vy, sqrt(c.rg * q.t), aa, bb, cc, dd, c.cfl * vol);
-            ratio_next[id] = (T)(vol / dl);
-            if (I.local_dt) I.ldt[id] = dl;
-            mloc = fmin(mloc, dl);
+            T aa = T(0.5) * ((T)gs[L::gTx + tdn] + (T)gs[L::gTx + tup]);
+            T bb = T(0.5) * ((T)gs[L::gTy + tdn] + (T)gs[L::gTy + tup]);
+            T cc = T(0.5) * ((T)gs[L::gNx + nlf] + (T)gs[L::gNx + nrt]);
+            T dd = T(0.5) * ((T)gs[L::gNy + nlf] + (T)gs[L::gNy + nrt]);
+            T vol = (T)gs[L::gV + w];
+            T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
+            T dl = local_dt<T>(qvx, qvy, sqrt((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
+            ratio_next[id] = vol / dl;
+            if (I.local_dt) I.ldt[id] = (double)dl;
+            mloc = fmin(mloc, (double)dl);
         }
     }
     if (LAST) {

@@ -15,8 +15,9 @@ Generators (all off the hot path, used to make inputs):
 * ``cylinder_o_mesh`` — a circular cylinder with a geometric radial distribution
   set by the first wall spacing and the far-field radius.
 * ``naca4_o_mesh`` — an algebraic O-mesh around a NACA 4-digit section (closed
-  trailing edge), cosine-clustered along the surface, straight radial lines to a
-  far-field circle, geometric radial stretching from a given wall spacing.
+  trailing edge), cosine-clustered along the surface, geometric radial
+  stretching from a given wall spacing, wall-normal extrusion near the wall
+  blended into straight lines to a far-field circle.
 """
 
 from __future__ import annotations
@@ -134,15 +135,37 @@ def naca4_surface(phi: np.ndarray, m: float, p: float, t: float, chord: float = 
     return chord * xs, chord * ys
 
 
+def _wall_normals(wx: np.ndarray, wy: np.ndarray, smooth: int) -> tuple[np.ndarray, np.ndarray]:
+    """Unit outward normals of a closed counter-clockwise wall polyline,
+    from central differences, then `smooth` passes of neighbour averaging
+    (periodic), which turns the normals gradually round a sharp trailing edge."""
+    tx = np.roll(wx, -1) - np.roll(wx, 1)
+    ty = np.roll(wy, -1) - np.roll(wy, 1)
+    nx, ny = ty, -tx
+    ln = np.hypot(nx, ny)
+    nx, ny = nx / ln, ny / ln
+    for _ in range(smooth):
+        nx = 0.25 * np.roll(nx, 1) + 0.5 * nx + 0.25 * np.roll(nx, -1)
+        ny = 0.25 * np.roll(ny, 1) + 0.5 * ny + 0.25 * np.roll(ny, -1)
+        ln = np.hypot(nx, ny)
+        nx, ny = nx / ln, ny / ln
+    return nx, ny
+
+
 def naca4_o_mesh(n_rings: int, n_theta: int, m: float = 0.0, p: float = 0.4, t: float = 0.12,
-                 chord: float = 1.0, r_far: float = 30.0, first_spacing: float = 1e-6) -> np.ndarray:
-    """Algebraic O-mesh around a NACA 4-digit section.  Open rings, CCW, ring 0 = wall.
+                 chord: float = 1.0, r_far: float = 30.0, first_spacing: float = 1e-6,
+                 orthogonal: bool = True, smooth: int = 8) -> np.ndarray:
+    """O-mesh around a NACA 4-digit section.  Open rings, CCW, ring 0 = wall.
 
     m, p, t are the camber, camber position and thickness as fractions of the
     chord (NACA 2412 -> m=0.02, p=0.4, t=0.12).  The far field is a circle of
-    radius r_far*chord around mid-chord; node (i, j) lies on the straight line
-    from wall point j to far-field point j at the geometric radial parameter
-    s_i, whose first step is first_spacing*chord over the nominal distance."""
+    radius r_far*chord around mid-chord.  Rings are placed at the geometric
+    radial parameter s_i (first step first_spacing*chord over the nominal
+    distance).  With `orthogonal`, node (i, j) blends a wall-normal extrusion
+    w_j + d_i n_j (smoothed normals, d_i the radial distance) with the straight
+    line from wall point j to far-field point j, weighted by s_i, so the wall
+    cells are nearly orthogonal and the trailing-edge cells are not slivers;
+    otherwise only the straight lines are used."""
     if n_rings < 4 or n_theta < 8:
         raise ValueError("an O-mesh needs at least 4 rings and 8 points per ring")
     phi = 2.0 * np.pi * np.arange(n_theta) / n_theta
@@ -150,9 +173,20 @@ def naca4_o_mesh(n_rings: int, n_theta: int, m: float = 0.0, p: float = 0.4, t: 
     cx = 0.5 * chord
     fx = cx + r_far * chord * np.cos(phi)
     fy = r_far * chord * np.sin(phi)
-    s = _radial_params(n_rings, first_spacing / (r_far - 0.5))
-    x = wx[None, :] + s[:, None] * (fx - wx)[None, :]
-    y = wy[None, :] + s[:, None] * (fy - wy)[None, :]
+    length = (r_far - 0.5) * chord
+    s = _radial_params(n_rings, first_spacing * chord / length)
+    bx = wx[None, :] + s[:, None] * (fx - wx)[None, :]
+    by = wy[None, :] + s[:, None] * (fy - wy)[None, :]
+    if orthogonal:
+        nx, ny = _wall_normals(wx, wy, smooth)
+        d = s * length
+        ax = wx[None, :] + d[:, None] * nx[None, :]
+        ay = wy[None, :] + d[:, None] * ny[None, :]
+        wgt = np.sqrt(s)[:, None]
+        x = (1.0 - wgt) * ax + wgt * bx
+        y = (1.0 - wgt) * ay + wgt * by
+    else:
+        x, y = bx, by
     return np.stack([x.ravel(), y.ravel()], axis=1)
 
 

@@ -42,12 +42,13 @@ FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
 EXPORTS = ["jst_default_opts", "jst_create_from_paths", "jst_create", "jst_destroy", "jst_last_error", "jst_ni",
            "jst_nj", "jst_advance", "jst_run", "jst_residual_terms", "jst_timestep", "jst_residual",
            "jst_totaltime", "jst_step_count", "jst_get_field", "jst_get_faces", "jst_set_conserved",
-           "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps", "jst_residual_noalloc"]
+           "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps", "jst_residual_noalloc", "jst_kernel_config"]
 
 
 class Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("dt_mode", C.c_int), ("kernel_path", C.c_int), ("device", C.c_int),
-                ("tile_i", C.c_int), ("tile_j", C.c_int), ("use_graph", C.c_int), ("nut_inf_ratio", C.c_double)]
+                ("tile_i", C.c_int), ("tile_j", C.c_int), ("use_graph", C.c_int), ("nut_inf_ratio", C.c_double),
+                ("block_threads", C.c_int)]
 
 
 class NonPhysicalC(C.Structure):
@@ -119,6 +120,7 @@ def lib() -> C.CDLL:
         L.jst_version.restype = C.c_char_p
         L.jst_time_steps.argtypes = [vp, i, pd, pd]
         L.jst_residual_noalloc.argtypes = [vp, vp, i, i, vp, vp]
+        L.jst_kernel_config.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.jst_debug_set_uniform.argtypes = [vp, d, d, d, d, d]
         L.jst_debug_kernel.argtypes = [vp, C.c_char_p]
         _lib = L
@@ -130,11 +132,12 @@ def _ptr(a: np.ndarray):
 
 
 def make_opts(precision=PREC_FP64, dt_mode=DT_GLOBAL, kernel_path=PATH_FUSED, device=0, tile_i=0, tile_j=0,
-              use_graph=1, nut_inf_ratio=0.0) -> Opts:
+              use_graph=1, nut_inf_ratio=0.0, block_threads=0) -> Opts:
     o = Opts()
     lib().jst_default_opts(C.byref(o))
     o.precision, o.dt_mode, o.kernel_path, o.device = precision, dt_mode, kernel_path, device
     o.tile_i, o.tile_j, o.use_graph, o.nut_inf_ratio = tile_i, tile_j, use_graph, nut_inf_ratio
+    o.block_threads = block_threads
     return o
 
 
@@ -278,6 +281,12 @@ class Solver:
         st = np.zeros(5)
         self._check(lib().jst_time_steps(self._h, int(nsteps), C.byref(ms), _ptr(st) if stages else None))
         return ms.value, (st.tolist() if stages else None)
+
+    def kernel_config(self):
+        """(tile_i, tile_j, block_threads) of the fused path (autotuned when not given)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(lib().jst_kernel_config(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     # test hooks
     def set_uniform(self, rho, vx, vy, p, nut):
