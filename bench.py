@@ -45,12 +45,13 @@ UNIT = "Mcell-stage/s"
 #          stages 2-4: U 40 + U_n 40 + write 40 + geom 56 + ratio 8       = 184
 #          stage 5: U 40 + U_n 40 + write U_n 40 + geom 56 + ratio 8+8    = 192
 #          average 177.6 B
-#   split: stage 1: U_n 40 + write 20 + geom 56 + ratio 4                 = 120
-#          stages 2-4: U 20 + U_n 40 + write 20 + geom 56 + ratio 4       = 140
-#          stage 5: U 20 + U_n 40 + write U_n 40 + geom 56 + ratio 4+4    = 164
-#          average 140.8 B
-BYTES_PER_CELL_STAGE = {"fp64": (144 + 3 * 184 + 192) / 5.0, "split": (120 + 3 * 140 + 164) / 5.0}
-BYTES_PER_STAGE = {"fp64": [144, 184, 184, 184, 192], "split": [120, 140, 140, 140, 164]}
+#   split (stage 1 reads the FP32 copy of U_n that stage 5 writes):
+#          stages 1-4: U 20 + U_n 40 + write 20 + geom 56 + ratio 4       = 140
+#          stage 5: U 20 + U_n 40 + write U_n 40 + FP32 copy 20 + geom 56
+#                   + ratio 4+4                                           = 184
+#          average 148.8 B
+BYTES_PER_CELL_STAGE = {"fp64": (144 + 3 * 184 + 192) / 5.0, "split": (4 * 140 + 184) / 5.0}
+BYTES_PER_STAGE = {"fp64": [144, 184, 184, 184, 192], "split": [140, 140, 140, 140, 184]}
 
 
 def measured_peaks():
@@ -286,12 +287,67 @@ def run_ours(args, world, rank, local):
                            "seconds": round(t_e2e, 4),
                            "what": "jst_create from host nodes + jst_run with per-step residual callback + "
                                    "6 fields read back"}
+        if world == 1 and args.batch_instances > 0:
+            line["batch"] = batched_leg(args)
         if world == 1 and not args.no_cpu:
             r = cpu_reference(args.workload, 2, 1)
             line["cpu_baseline"] = {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
                                     "sample": f"{args.workload}: {r['cells']} cells, 1 untimed + 2 timed RK steps, "
                                               f"oracle (CPU FP64 restatement of jst-rs), {r['cores']} threads"}
         print(json.dumps(line), flush=True)
+
+
+def batched_leg(args):
+    """Config-4 distribution: NACA 4-digit instances on three mesh classes with
+    seeded M, alpha, Re (local time stepping, CFL 1.0), solved (a) all at once
+    in one FP32-split batch, (b) all at once in FP64 as the CL/CD reference and
+    (c) a subsample one at a time in FP64 (batch of one).  Each instance
+    retires on a 1e-6 residual drop or at the step cap."""
+    from purinecfd_b200 import PREC_FP32_SPLIT, PREC_FP64, workloads
+    from purinecfd_b200.serve import batch_solve, percentile
+    cases = []
+    for k in range(args.batch_instances):
+        cfg, xy, nr, nt, _ = workloads.batch_instance(20261203, k)
+        cfg["simulation"]["CFL"] = 1.0
+        cases.append((cfg, xy, nr, nt))
+    cells = sum((c[2] - 1) * c[3] for c in cases)
+    split, t_split = batch_solve(cases, PREC_FP32_SPLIT, max_steps=args.batch_steps)
+    ref, t_ref = batch_solve(cases, PREC_FP64, max_steps=args.batch_steps)
+    m = max(1, min(args.plain_instances, len(cases)))
+    plain, t_plain = batch_solve(cases[:m], PREC_FP64, max_instances=1, max_steps=args.batch_steps)
+    dcl, dcd = [], []
+    for a, r in zip(split, ref):
+        if a.status != 8 and r.status != 8:
+            dcl.append(abs(a.cl - r.cl))
+            dcd.append(abs(a.cd - r.cd))
+    within = sum(1 for x, y in zip(dcl, dcd) if x <= 1e-4 and y <= 1e-4)
+    lat = [r.t_done - r.t_submit for r in split]
+    steps_split = sum(r.steps for r in split)
+    return {"instances": len(cases), "cells": cells, "step_cap": args.batch_steps,
+            "solves_per_s": round(len(cases) / t_split, 3), "wall_s": round(t_split, 3),
+            "mcell_stage_per_s": round(sum((r.ni * r.nj) * r.steps for r in split) * 5 / t_split / 1e6, 1),
+            "p50_s": round(percentile(lat, 50), 3), "p99_s": round(percentile(lat, 99), 3),
+            "converged": sum(1 for r in split if r.status == 0), "nonphysical": sum(1 for r in split if r.status == 8),
+            "mean_steps": round(steps_split / len(split), 1),
+            "fp64_batch_solves_per_s": round(len(cases) / t_ref, 3),
+            "plain_fp64_one_at_a_time": {"instances": m, "solves_per_s": round(m / t_plain, 3),
+                                         "wall_s": round(t_plain, 3)},
+            "speedup_vs_plain": round((len(cases) / t_split) / (m / t_plain), 2),
+            "cl_err_max": max(dcl) if dcl else None, "cd_err_max": max(dcd) if dcd else None,
+            "within_1e-4": f"{within}/{len(cases)}",
+            "what": "seed 20261203, PCG64 stream per instance; local time step; retire at residual drop 1e-6 "
+                    "or step cap; CL/CD error vs the FP64 batch on the same instances"}
+
+
+def serve_sweep(args):
+    from purinecfd_b200.serve import request_stream, serve
+    out = []
+    for rate in [float(x) for x in args.serve_rates.split(",")]:
+        reqs = request_stream(20261203, args.serve_requests, max_steps=args.batch_steps)
+        st, _ = serve(reqs, rate, seed=int(rate))
+        out.append(st.__dict__)
+        print(json.dumps({"serve": st.__dict__}), flush=True)
+    return out
 
 
 def main():
@@ -306,12 +362,21 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain-path line")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--batch-instances", type=int, default=256, help="config-4 batch size (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=1000, help="step cap per batched instance")
+    ap.add_argument("--plain-instances", type=int, default=8, help="FP64 one-at-a-time subsample")
+    ap.add_argument("--serve", action="store_true", help="run the serving sweep instead of the benchmark")
+    ap.add_argument("--serve-rates", default="1,10,50,200")
+    ap.add_argument("--serve-requests", type=int, default=64)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                    int(os.environ.get("RANK", "0")), 0)
     try:
+        if args.serve:
+            serve_sweep(args)
+            return
         if args.impl == "reference":
             run_reference(args, world, rank)
         else:

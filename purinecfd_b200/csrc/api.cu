@@ -81,6 +81,7 @@ PhysConst make_phys(const RawConfig& r) {
     c.inv_kappa2 = 1.0 / (r.kappa * r.kappa);
     c.cw3_6 = powi6(r.Cw3);
     c.one_plus_cw3_6 = 1.0 + powi6(r.Cw3);
+    c.fw_lim = std::pow(c.one_plus_cw3_6, 1.0 / 6.0);
     c.gm1 = r.gamma - 1.0;
     c.rg = r.r_gas * r.gamma;
     c.gm1_q = (r.gamma - 1.0) / 4.0;

@@ -158,11 +158,20 @@ JST_D Prim<T> prim_from(const TS* const* src, long idx, int fresh, const PhysCon
 }
 
 // Block-wide reduction helpers over NT threads (fixed shape: deterministic).
+// Largest power of two not above n: block sizes of 192 or 384 threads first
+// fold their upper part onto it, so that the tree below sees every element.
+JST_HD constexpr int pow2_floor(int n) { return n < 2 ? 1 : 2 * pow2_floor(n / 2); }
+
 template <int NT> JST_D double block_sum(double v, double* red) {
+    constexpr int P = pow2_floor(NT);
     int t = JST_TID();
     red[t] = v;
     JST_SYNC();
-    for (int w = NT / 2; w > 0; w >>= 1) {
+    if (P < NT) {
+        if (t < NT - P) red[t] += red[t + P];
+        JST_SYNC();
+    }
+    for (int w = P / 2; w > 0; w >>= 1) {
         if (t < w) red[t] += red[t + w];
         JST_SYNC();
     }
@@ -172,10 +181,15 @@ template <int NT> JST_D double block_sum(double v, double* red) {
 }
 
 template <int NT> JST_D double block_min(double v, double* red) {
+    constexpr int P = pow2_floor(NT);
     int t = JST_TID();
     red[t] = v;
     JST_SYNC();
-    for (int w = NT / 2; w > 0; w >>= 1) {
+    if (P < NT) {
+        if (t < NT - P) red[t] = fmin(red[t], red[t + P]);
+        JST_SYNC();
+    }
+    for (int w = P / 2; w > 0; w >>= 1) {
         if (t < w) red[t] = fmin(red[t], red[t + w]);
         JST_SYNC();
     }
@@ -576,8 +590,12 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
             int o = cl * LJ + lj;
             for (int q = 0; q < 4; ++q) {
                 const T* f = sQ + q * NL;
-                green_gauss<T>(f[o], f[o + LJ], f[o - LJ], f[o - 1], f[o + 1], upx, upy, dnx, dny, lfx, lfy, rtx,
-                               rty, iv, &g[2 * q], &g[2 * q + 1]);
+                if (sizeof(T) == sizeof(double))
+                    green_gauss<T>(f[o], f[o + LJ], f[o - LJ], f[o - 1], f[o + 1], upx, upy, dnx, dny, lfx, lfy, rtx,
+                                   rty, iv, &g[2 * q], &g[2 * q + 1]);
+                else
+                    green_gauss_delta<T>(f[o], f[o + LJ], f[o - LJ], f[o - 1], f[o + 1], upx, upy, dnx, dny, lfx,
+                                         lfy, rtx, rty, iv, &g[2 * q], &g[2 * q + 1]);
             }
             if (gi < 0) {
                 g[4] = T(0);
@@ -606,6 +624,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
     JST_SYNC();
 
     const T half_cfl = (T)c.half_cfl, k2 = (T)c.k2, k4 = (T)c.k4, gm1 = (T)c.gm1;
+    const T p_ref = sizeof(T) == sizeof(double) ? T(0) : (T)c.p_inf;  // see euler_flux
 
     // ---- C: net face fluxes G = conv - visc - diss, each face once -------
     T* sFt = sm + L::oX;               // tau faces i0 .. i0+TI (aliases the dead P, Q)
@@ -648,7 +667,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* n
         lam = half_cfl * (sRat[db] + sRat[da]);
         T fu[5], cv[5];
         for (int k = 0; k < 5; ++k) fu[k] = T(0.5) * (sU[k * NL + lo - step] + sU[k * NL + lo]);
-        euler_flux<T>(fu, nx, ny, gm1, cv);
+        euler_flux<T>(fu, nx, ny, gm1, cv, p_ref);
         T hx = T(0.5) * nx, hy = T(0.5) * ny;
         T* out = tau ? sFt + w : sFn + (w - L::NFT);
         const int ostride = tau ? L::NFT : L::NFN;

@@ -41,6 +41,7 @@ struct PhysConst {
     double cb1_k2;       // Cb1 * inv_kappa2             source.rs:52
     double cb2_sigma;    // Cb2 * sigma                  source.rs:53
     double r_gas_gamma;  // r_gas * gamma                boundary.rs:139 (c^2/(r_gas*gamma))
+    double fw_lim;       // (1 + Cw3^6)^(1/6), the limit of fw for large g
     int supersonic;
     int halo;
     // Free-stream primitive state written by Cells::initialize (state.rs:522-539).
@@ -98,7 +99,12 @@ template <class T> JST_HD T mu_of(T t, T inv_t_ref, T suth_num, T t_suth) {
 }
 
 // convection::euler_flux (convection.rs:25-40): F.n of the face state fu.
-template <class T> JST_HD void euler_flux(const T fu[5], T nx, T ny, T gm1, T out[5]) {
+// p_ref is subtracted from the pressure in the momentum flux only: with
+// closed metrics (sum of n over a cell = 0) the cell sums are unchanged, and
+// in FP32 the large constant part of p no longer cancels between the two
+// faces of a thin wall cell.  The FP64 paths pass p_ref = 0, i.e. the
+// reference's formula.
+template <class T> JST_HD void euler_flux(const T fu[5], T nx, T ny, T gm1, T out[5], T p_ref = T(0)) {
     T rho = fu[0];
     T inv_rho = T(1) / rho;
     T u = fu[1] * inv_rho;
@@ -106,9 +112,10 @@ template <class T> JST_HD void euler_flux(const T fu[5], T nx, T ny, T gm1, T ou
     T rho_e = fu[3];
     T p = gm1 * (rho_e - rho * (u * u + v * v) * T(0.5));
     T vn = nx * u + ny * v;
+    T pm = p - p_ref;
     out[0] = rho * vn;
-    out[1] = fu[1] * vn + p * nx;
-    out[2] = fu[2] * vn + p * ny;
+    out[1] = fu[1] * vn + pm * nx;
+    out[2] = fu[2] * vn + pm * ny;
     out[3] = (rho_e + p) * vn;
     out[4] = fu[4] * vn;
 }
@@ -125,6 +132,20 @@ JST_HD void green_gauss(T c, T vup, T vdn, T vlf, T vrt, T upx, T upy, T dnx, T 
     T f_rt = T(0.5) * (c + vrt);
     *gx = (f_up * upx - f_dn * dnx + f_rt * rtx - f_lf * lfx) * inv_v;
     *gy = (f_up * upy - f_dn * dny + f_rt * rty - f_lf * lfy) * inv_v;
+}
+
+// The same Green-Gauss sum in difference form, sum_f 0.5 (phi_nb - phi_c) n_f / V:
+// identical to green_gauss when the cell's metrics close (sum of n = 0), and
+// free of the cancellation of c * sum(n) in FP32.  Used by the FP32 path.
+template <class T>
+JST_HD void green_gauss_delta(T c, T vup, T vdn, T vlf, T vrt, T upx, T upy, T dnx, T dny, T lfx, T lfy, T rtx,
+                              T rty, T inv_v, T* gx, T* gy) {
+    T d_up = T(0.5) * (vup - c);
+    T d_dn = T(0.5) * (vdn - c);
+    T d_lf = T(0.5) * (vlf - c);
+    T d_rt = T(0.5) * (vrt - c);
+    *gx = (d_up * upx - d_dn * dnx + d_rt * rtx - d_lf * lfx) * inv_v;
+    *gy = (d_up * upy - d_dn * dny + d_rt * rty - d_lf * lfy) * inv_v;
 }
 
 // Diffusion tensor columns of one cell (viscous.rs:37-71): returns mu, chi,
@@ -177,6 +198,19 @@ template <class T> JST_HD T fw_of(T r, T cw2, T cw3_6, T one_plus_cw3_6) {
     return g * cbrt(sqrt(one_plus_cw3_6 / (powi6<T>(g) + cw3_6)));
 }
 
+// fw for the FP32 path.  Near the wall a slightly negative nu-tilde over
+// d^2 ~ 1e-12 makes |r| reach 1e7 and more; r^6 then overflows FP32 and the
+// reference formula would give inf * 0 = NaN, where FP64 still evaluates it
+// (to (1 + Cw3^6)^(1/6) within rounding once g^6 dwarfs Cw3^6).  So g is
+// formed in FP64 and, beyond g = 1e5, fw takes that limit.
+JST_HD float fw_of_f32(float r, double cw2, double cw3_6, double one_plus_cw3_6, double fw_lim) {
+    double rd = (double)r;
+    double g = rd + cw2 * (powi6<double>(rd) - rd);
+    if (g > 1e5) return (float)fw_lim;
+    float gf = (float)g;
+    return gf * cbrt(sqrt((float)one_plus_cw3_6 / (powi6<float>(gf) + (float)cw3_6)));
+}
+
 // source::compute for one cell (source.rs:55-85), before the factor V.
 template <class T>
 JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny, const PhysConst& c) {
@@ -188,8 +222,10 @@ JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T 
     T s_tilde = tmax<T>(sv + nu_tilde * inv_kd2 * fv2, T(1e-10));
     T prod = T(c.Cb1) * (T(1) - ft2) * s_tilde * rho_nu;
     T r = tmin<T>(nu_tilde / s_tilde * inv_kd2, T(c.rmax));
-    T destr = (T(c.cw1) * fw_of<T>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6)) - T(c.cb1_k2) * ft2) * rho *
-              (nu_tilde * nu_tilde * inv_dist2);
+    T fw;
+    if constexpr (sizeof(T) == sizeof(float)) fw = fw_of_f32(r, c.Cw2, c.cw3_6, c.one_plus_cw3_6, c.fw_lim);
+    else fw = fw_of<T>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6));
+    T destr = (T(c.cw1) * fw - T(c.cb1_k2) * ft2) * rho * (nu_tilde * nu_tilde * inv_dist2);
     T diff = T(c.cb2_sigma) * rho * (dnx * dnx + dny * dny);
     return prod - destr + diff;
 }

@@ -78,6 +78,24 @@ def test_fused_tile_shape_invariance_bitwise(tile):
         assert np.array_equal(a.get(f"U{k}"), b.get(f"U{k}")), k
 
 
+@pytest.mark.parametrize("cfgt", [(4, 32, 256), (8, 32, 128), (8, 32, 192), (16, 32, 384), (8, 64, 256)],
+                         ids=lambda t: "x".join(map(str, t)))
+def test_fused_every_compiled_configuration_matches_oracle(cfgt):
+    """Every tile shape and block size the autotuner may pick (block sizes
+    that are not powers of two included) reproduces the oracle's residual
+    history, global time step and fields."""
+    cfg, xy, nr, nt = cylinder_case(33, 64)
+    s = _solver(cfg, xy, nr, nt, tile_i=cfgt[0], tile_j=cfgt[1], block_threads=cfgt[2])
+    o = jo.OracleSolver(cfg, xy, nr, nt)
+    hist = []
+    s.run(30, lambda k, r: hist.append(r))
+    _, _, _, _, hist_o = o.run(30, history=True)
+    np.testing.assert_allclose(hist, hist_o, rtol=1e-10)
+    assert abs(s.totaltime - o.totaltime) <= 1e-12 * o.totaltime
+    for name in STATE_FIELDS:
+        assert rel_field_err(s.get(name), o.get(name)) < 1e-10, name
+
+
 def test_fused_run_to_run_bitwise():
     cfg, xy, nr, nt = cylinder_case(33, 64)
     runs = []
