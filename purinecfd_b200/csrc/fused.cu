@@ -23,6 +23,7 @@
 #include "config_mesh.h"
 #include "engine.h"
 #include "fused_kernels.cuh"
+#include "march_kernels.cuh"
 
 namespace jst {
 
@@ -144,12 +145,17 @@ void launch_wall_force(const Geom& g, const UnPtrs& up, const PhysConst& c, doub
 
 // Tile configurations compiled into the library: (TI, TJ, NT).
 #define JST_FOR_TILES(X) X(4, 32, 256) X(8, 32, 256) X(16, 32, 256) X(4, 64, 256) X(8, 64, 256) X(8, 32, 192) X(8, 32, 128) X(16, 32, 384)
+// Marching-strip configurations: (rows per strip H, threads per block).  A
+// strip is fused::MARCH_W = 26 columns wide, so these are selected by
+// tile_j == 26, tile_i == H.
+#define JST_FOR_MARCH(X) X(16, 128) X(32, 128) X(64, 128) X(32, 256) X(32, 64)
 
 template <class T> struct Kernels {
-    void (*stage[3])(const TileRef*, const int*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};
+    void (*stage[3])(const TileRef*, int*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};
     void (*step_dt)(const TileRef*, const int*, const Inst<T>*, int, int) = nullptr;
     size_t smem = 0;
     int nt = 256;
+    bool march = false;  // warp per work item (else block per tile)
 };
 
 template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
@@ -163,6 +169,18 @@ template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
     return k;
 }
 
+template <class T, int H, int NT> Kernels<T> march_kernels_for() {
+    Kernels<T> k;
+    k.stage[0] = fused::k_march<T, H, NT, true, false>;
+    k.stage[1] = fused::k_march<T, H, NT, false, false>;
+    k.stage[2] = fused::k_march<T, H, NT, false, true>;
+    k.step_dt = fused::k_step_dt<T, NT>;
+    k.smem = 0;
+    k.nt = NT;
+    k.march = true;
+    return k;
+}
+
 template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 256) {
 #define JST_PICK(a, b, n)                               \
     if (ti == a && tj == b && nt == n) {                \
@@ -171,7 +189,24 @@ template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 2
     }
     JST_FOR_TILES(JST_PICK)
 #undef JST_PICK
+#define JST_PICK_MARCH(h, n)                                        \
+    if (ti == h && tj == fused::MARCH_W && nt == n) {               \
+        *out = march_kernels_for<T, h, n>();                        \
+        return true;                                                \
+    }
+    JST_FOR_MARCH(JST_PICK_MARCH)
+#undef JST_PICK_MARCH
     return false;
+}
+
+// Grid of a stage launch over `items` work items: one block per tile for the
+// tile kernels; for the marching kernels enough blocks to give every strip a
+// warp, at most the resident limit (warps take strips from a work counter).
+template <class T> int stage_grid(const Kernels<T>& K, int items, int resident_blocks) {
+    if (!K.march) return std::max(1, items);
+    int wpb = K.nt / 32;
+    int need = (items + wpb - 1) / wpb;
+    return std::max(1, std::min(need, std::max(1, resident_blocks)));
 }
 
 // Default tile per precision and mesh width (the autotuner refines this).
@@ -186,8 +221,10 @@ void default_tile(int prec, int nj, int* ti, int* tj) {
 }
 
 // Tile configurations the autotuner times, in order (TI, TJ, threads).
+// Marching candidates are (H, 26, threads).
 const int kTileCands[][3] = {{8, 32, 256}, {8, 32, 192}, {16, 32, 384}, {16, 32, 256}, {4, 32, 256},
-                             {4, 64, 256},  {8, 64, 256}, {8, 32, 128}};
+                             {4, 64, 256},  {8, 64, 256}, {8, 32, 128}, {32, 26, 128}, {16, 26, 128},
+                             {64, 26, 128}, {32, 26, 64}};
 
 // Stage input buffer = T copy of U_n, so a middle stage can be timed without
 // touching the solution.
@@ -244,14 +281,18 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
             if (d_t) cudaFree(d_t);
             cap = tiles.size();
             cudaMalloc(&d_t, cap * sizeof(TileRef) + 256);
-            if (!d_n) cudaMalloc(&d_n, sizeof(int));
+            if (!d_n) {
+                cudaMalloc(&d_n, 4 * sizeof(int));  // strip count + the marching kernels' work counters
+                cudaMemsetAsync(d_n, 0, 4 * sizeof(int), st);
+            }
         }
         int nt_ = (int)tiles.size();
         cudaMemcpyAsync(d_t, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(d_n, &nt_, sizeof(int), cudaMemcpyHostToDevice, st);
         int occ = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K.stage[1], K.nt, K.smem);
-        int grid = grid_hint > 0 ? std::min(nt_, sms * std::max(1, occ)) : nt_;
+        int grid = K.march ? stage_grid(K, nt_, sms * std::max(1, occ))
+                           : (grid_hint > 0 ? std::min(nt_, sms * std::max(1, occ)) : nt_);
         JST_LAUNCH(K.stage[1], grid, K.nt, K.smem, st, d_t, d_n, d_insts, 1, RK_ALPHA[1]);  // warm-up
         cudaEventRecord(e0, st);
         for (int r = 0; r < 3; ++r) JST_LAUNCH(K.stage[1], grid, K.nt, K.smem, st, d_t, d_n, d_insts, 1, RK_ALPHA[1]);
@@ -298,10 +339,17 @@ template <class T> class FusedEngine : public Engine {
                 err = "stage kernel needs " + std::to_string(K_.smem) + " bytes of shared memory";
                 return false;
             }
+        int dev = 0, sms = 148, occ = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K_.stage[1], K_.nt, K_.smem);
+        resident_ = sms * std::max(1, occ);
         ti_ = ti;
         tj_ = tj;
         return true;
     }
+
+    int sgrid() const { return stage_grid(K_, ntiles_, resident_); }
 
     bool create(std::string& err) {
         SolverCore& C = *core_;
@@ -470,7 +518,7 @@ template <class T> class FusedEngine : public Engine {
     void enqueue_step(cudaStream_t st) {
         for (int s = 0; s < 5; ++s) {
             auto kern = s == 0 ? K_.stage[0] : (s == 4 ? K_.stage[2] : K_.stage[1]);
-            JST_LAUNCH(kern, ntiles_, K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, s, RK_ALPHA[s]);
+            JST_LAUNCH(kern, sgrid(), K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, s, RK_ALPHA[s]);
         }
     }
 
@@ -732,7 +780,7 @@ template <class T> class FusedEngine : public Engine {
             cudaEventRecord(ev[2], st);
             for (int q = 0; q < 5; ++q) {
                 auto kern = q == 0 ? K_.stage[0] : (q == 4 ? K_.stage[2] : K_.stage[1]);
-                JST_LAUNCH(kern, ntiles_, K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, q, RK_ALPHA[q]);
+                JST_LAUNCH(kern, sgrid(), K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, q, RK_ALPHA[q]);
                 cudaEventRecord(ev[3 + q], st);
             }
         }
@@ -756,7 +804,7 @@ template <class T> class FusedEngine : public Engine {
   private:
     SolverCore* core_;
     Kernels<T> K_;
-    int ti_ = 8, tj_ = 32, ntiles_ = 0;
+    int ti_ = 8, tj_ = 32, ntiles_ = 0, resident_ = 148;
     bool tune_ = false;
     void* arena_ = nullptr;
     double* extra_hist_ = nullptr;

@@ -317,7 +317,7 @@ JST_D void async_wait_all() {
 // The stage kernel.  FIRST: stage 0 (reads U_n, adds dt to the total time).
 // LAST: stage 4 (writes U_n in place, residual, next step's time step).
 template <class T, int TI, int TJ, int NT, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, const int* ntiles, const Inst<T>* insts, int stage,
+__global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles, const Inst<T>* insts, int stage,
                                               double alpha) {
     using L = Layout<T, TI, TJ, NT>;
     // Stage 0 reads U_n; in the split mode it stages the T copy of U_n that the

@@ -1,0 +1,505 @@
+// Warp-marching stage kernel: the same RK stage as k_stage (fused_kernels.cuh),
+// organised for instruction economy instead of shared-memory tiles.
+//
+// Work item = a strip of 26 output columns (j0 .. j0+25) and up to H rows
+// (i0 .. i0+H-1) of one instance.  One warp owns a strip: lane L holds column
+// j0-3+L (a 3-column halo on each side), so every j-neighbour the stencil
+// needs is one or two lanes away and comes from a register shuffle; the warp
+// walks down the rows i0-3 .. i0+H+2 keeping sliding windows of the rows it
+// still needs in registers (U: 4 rows, primitives: 2, sensors: 3, diffusion
+// tensors: 2, the previous tau-face flux).  Every value is loaded from HBM
+// once per strip and computed once per cell (plus a 6-row warm-up and the
+// 6-lane halo), no block barrier is used, and warps take strips from a
+// per-launch work counter so uneven instances balance.
+//
+// Per row k of the walk (rows lag so that each input is ready):
+//   load U(k) -> primitives, j-sensor(k);  i-sensor(k-1);
+//   gradients + diffusion tensor + SA source of row k-1;
+//   tau face k-2;  n faces of row k-3 and the RK update of row k-3.
+// The arithmetic of every term is the one k_stage uses (shared helpers in
+// jst_common.cuh), in the same operation order.
+#pragma once
+
+#ifndef JST_LANE
+#define JST_LANE() ((int)(threadIdx.x & 31))
+#define JST_WARP_IN_BLOCK() ((int)(threadIdx.x >> 5))
+template <class V> __device__ __forceinline__ V jst_shfl_up(V v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+template <class V> __device__ __forceinline__ V jst_shfl_down(V v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+template <class V> __device__ __forceinline__ V jst_shfl_xor(V v, int d) { return __shfl_xor_sync(0xffffffffu, v, d); }
+template <class V> __device__ __forceinline__ V jst_shfl_idx(V v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+#endif
+
+namespace jst {
+namespace fused {
+
+constexpr int MARCH_W = 26;  // output columns per strip (32 lanes - 2 x 3 halo)
+
+template <class V> JST_D V warp_sum0(V v) {  // lane 0 gets a fixed-order sum
+    for (int o = 16; o > 0; o >>= 1) v += jst_shfl_xor(v, o);
+    return v;
+}
+template <class V> JST_D V warp_min(V v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, jst_shfl_xor(v, o));
+    return v;
+}
+
+// Last-warp-done reduction of the per-strip partials (the warp version of
+// finish_step): dt and, when `with_residual`, the residual of the step.
+template <class T> JST_D void finish_step_warp(const Inst<T>& I, bool with_residual) {
+    const int lane = JST_LANE();
+    double m = __longlong_as_double(0x7ff0000000000000LL);
+    double s = 0.0;
+    for (int k = lane; k < I.ntiles; k += 32) {
+        volatile const double* pp = I.partial + 2 * k;
+        m = fmin(m, pp[0]);
+        s += pp[1];
+    }
+    double mn = warp_min(m);
+    double sm = warp_sum0(s);
+    if (lane == 0) {
+        InstState* st = I.st;
+        st->dt = mn;
+        if (with_residual) {
+            double res = sqrt(sm / (double)I.ni / (double)I.nj);
+            int step = st->step;
+            st->residual = res;
+            if (I.res_hist) I.res_hist[step] = res;
+            if (step == 0) st->res_first = res;
+            st->step = step + 1;
+            st->fresh = 0;
+            if (res < st->target || (st->drop > 0.0 && res < st->drop * st->res_first)) st->done = 1;
+        }
+        st->counter = 0;
+    }
+}
+
+// sched[0] = number of strips, sched[1] = work counter, sched[2] = exit counter
+// (both zero at launch; the last warp to leave resets them).
+template <class T, int H, int NT, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage,
+                                              double alpha) {
+    using TD = typename std::conditional<LAST, double, T>::type;
+    const int lane = JST_LANE();
+    const int nt_all = sched[0];
+    unsigned* work = reinterpret_cast<unsigned*>(sched + 1);
+    unsigned* exitc = reinterpret_cast<unsigned*>(sched + 2);
+    const unsigned nwarps = (unsigned)JST_GRID() * (NT / 32);
+    for (;;) {
+        unsigned ticket = 0;
+        if (lane == 0) ticket = atomicAdd(work, 1u);
+        ticket = jst_shfl_idx(ticket, 0);
+        if (ticket >= (unsigned)nt_all) {
+            if (lane == 0 && atomicAdd(exitc, 1u) == nwarps - 1) {
+                *work = 0u;
+                *exitc = 0u;
+            }
+            break;
+        }
+        const TileRef tr = tiles[ticket];
+        const Inst<T>& I = insts[tr.inst];
+        const int ni = I.ni, nj = I.nj, i0 = tr.i0, j0 = tr.j0;
+        const PhysConst& c = I.c;
+
+        int hdr[3] = {0, 0, 0};  // skip, fresh, step
+        if (lane == 0) {
+            InstState* st = I.st;
+            int step = st->step;
+            unsigned long long sid = (unsigned long long)step * 5 + stage;
+            unsigned long long bad = st->bad;
+            hdr[0] = st->done || step >= st->max_step || (bad != NO_BAD && (bad >> 32) < sid);
+            hdr[1] = FIRST ? st->fresh : 0;
+            hdr[2] = step;
+            if (FIRST && !hdr[0] && tr.tile == 0) st->totaltime += st->dt;
+        }
+        const int skip = jst_shfl_idx(hdr[0], 0);
+        if (skip) continue;
+        const int fresh = jst_shfl_idx(hdr[1], 0);
+        const int step = jst_shfl_idx(hdr[2], 0);
+        const unsigned long long stage_id = (unsigned long long)step * 5 + stage;
+        const T* ratio = I.ratio[step & 1];
+        T* ratio_next = I.ratio[(step + 1) & 1];
+        (void)ratio_next;
+        const T* src[5];
+        TD* dst[5];
+        for (int v = 0; v < 5; ++v) {
+            if (FIRST) src[v] = sizeof(T) == sizeof(double) ? reinterpret_cast<const T*>(I.un[v]) : I.uc[v];
+            else src[v] = (stage % 2 == 1) ? I.ua[v] : I.ub[v];
+            if (LAST) dst[v] = reinterpret_cast<TD*>(I.un[v]);
+            else dst[v] = reinterpret_cast<TD*>((stage % 2 == 0) ? I.ua[v] : I.ub[v]);
+        }
+
+        const int i1 = i0 + H < ni ? i0 + H : ni;  // output rows i0 .. i1-1
+        const int cu = j0 - 3 + lane;               // unwrapped column of this lane
+        const int gj = wrapj(cu, nj);
+        const bool seam = cu < 0 || cu >= nj;
+        const bool out_lane = lane >= 3 && lane < 3 + MARCH_W && cu < nj;
+        const T gm1 = (T)c.gm1, rgas = (T)c.r_gas;
+        const T half_cfl = (T)c.half_cfl, k2 = (T)c.k2, k4 = (T)c.k4;
+        const T p_ref = sizeof(T) == sizeof(double) ? T(0) : (T)c.p_inf;  // see euler_flux
+
+        // sliding windows (index 0 = oldest row)
+        T u[4][5];      // U rows k-4 .. k-1
+        T pw[2];        // p rows k-2, k-1
+        T qw[2][4];     // (vx, vy, T, nut) rows k-2, k-1
+        T nu3 = T(0);   // nut row k-3 (far-field extrapolation)
+        T si[3];        // i-sensor rows k-4 .. k-2
+        T sj[3];        // j-sensor rows k-3 .. k-1
+        T dw[2][8];     // diffusion tensor rows k-3, k-2
+        T sw[2];        // SA source * V rows k-3, k-2
+        T rt0 = T(0);   // V/dt row k-3 (rows clamped to the mesh)
+        T ft[5];        // tau-face flux of face k-3
+        T tx[3], ty[3]; // tau normals rows k-3 .. k-1
+        T nx2[2], ny2[2];  // n normals (left face of this column) rows k-3, k-2
+        for (int a = 0; a < 4; ++a)
+            for (int v = 0; v < 5; ++v) u[a][v] = T(0);
+        for (int a = 0; a < 2; ++a) {
+            pw[a] = T(0);
+            sw[a] = T(0);
+            nx2[a] = ny2[a] = T(0);
+            for (int v = 0; v < 4; ++v) qw[a][v] = T(0);
+            for (int v = 0; v < 8; ++v) dw[a][v] = T(0);
+        }
+        for (int a = 0; a < 3; ++a) {
+            si[a] = sj[a] = T(0);
+            tx[a] = ty[a] = T(0);
+        }
+        for (int v = 0; v < 5; ++v) ft[v] = T(0);
+        double mloc = __longlong_as_double(0x7ff0000000000000LL);
+        double sres = 0.0;
+
+        for (int k = i0 - 3; k <= i1 + 2; ++k) {
+            // ---- row k: conserved state and primitives ---------------------
+            T uk[5], pk, qk[4];
+            if (k < ni) {
+                const bool wall = k < 0;
+                const int kr = wall ? -1 - k : k;  // the wall ghost mirrors cell -1-k (boundary.rs:30-51)
+                const long id = (long)kr * nj + gj;
+                for (int v = 0; v < 5; ++v) uk[v] = ld(src[v] + id);
+                Prim<T> p;
+                if (fresh) {
+                    p.rho = (T)c.f_rho;
+                    p.p = (T)c.f_p;
+                    p.t = (T)c.f_t;
+                    p.vx = (T)c.f_vx;
+                    p.vy = (T)c.f_vy;
+                    p.e = (T)c.f_e;
+                    p.nut = (T)c.f_nut;
+                } else {
+                    p = unpack_cell<T>(uk[0], uk[1], uk[2], uk[3], uk[4], gm1, rgas);
+                }
+                if (seam) pack_cell<T>(p, uk);  // periodic ghost column (boundary.rs:54-72)
+                if (wall) {
+                    Prim<T> q;
+                    q.rho = uk[0];
+                    q.p = p.p;
+                    q.t = p.t;
+                    q.vx = -p.vx;
+                    q.vy = -p.vy;
+                    q.nut = -p.nut;
+                    q.e = fresh ? (T)c.f_e : uk[3] * (T(1) / q.rho);
+                    pack_cell<T>(q, uk);
+                    p = q;
+                }
+                pk = p.p;
+                qk[0] = p.vx;
+                qk[1] = p.vy;
+                qk[2] = p.t;
+                qk[3] = p.nut;
+            } else if (k == ni) {  // far-field ghost rows (boundary.rs:87-155), all three alike
+                const double* fg = I.far + 5 * (long)gj;
+                double nu[3] = {(double)qw[1][3], (double)qw[0][3], (double)nu3};
+                double dist[3] = {ld(fg + 2), ld(fg + 3), ld(fg + 4)};
+                double t = (double)qw[1][2];
+                double cs = fresh ? c.f_c : sqrt(c.rg * t);
+                FarState f = riemann_face(ld(fg + 0), ld(fg + 1), (double)qw[1][0], (double)qw[1][1], cs, dist, nu, c);
+                Prim<T> q;
+                q.rho = (T)f.rho;
+                q.p = (T)f.p;
+                q.t = (T)f.t;
+                q.vx = (T)f.vx;
+                q.vy = (T)f.vy;
+                q.e = (T)f.e;
+                q.nut = (T)f.nut;
+                pack_cell<T>(q, uk);
+                pk = q.p;
+                qk[0] = q.vx;
+                qk[1] = q.vy;
+                qk[2] = q.t;
+                qk[3] = q.nut;
+            } else {  // rows ni+1, ni+2 repeat row ni
+                for (int v = 0; v < 5; ++v) uk[v] = u[3][v];
+                pk = pw[1];
+                for (int v = 0; v < 4; ++v) qk[v] = qw[1][v];
+            }
+            // j-sensor of row k (dissipation.rs:73-90)
+            const T sjk = pressure_sensor<T>(jst_shfl_up(pk, 1), pk, jst_shfl_down(pk, 1));
+            // i-sensor of row k-1
+            const T sik = pressure_sensor<T>(pw[0], pw[1], pk);
+
+            // ---- tau normals of face row k ---------------------------------
+            T txk = T(0), tyk = T(0);
+            if (k >= 0 && k <= ni) {
+                long f = (long)k * nj + gj;
+                txk = (T)ld(I.tnx + f);
+                tyk = (T)ld(I.tny + f);
+            }
+
+            // ---- gradients, diffusion tensor, SA source of row r = k-1 -----
+            const int r = k - 1;
+            T dn[8];
+            for (int v = 0; v < 8; ++v) dn[v] = T(0);
+            T snew = T(0), nxr = T(0), nyr = T(0);
+            if (r >= i0 - 1 && r <= i1) {
+                if (r >= 0 && r < ni) {
+                    const long id = (long)r * nj + gj;
+                    nxr = (T)ld(I.nnx + id);
+                    nyr = (T)ld(I.nny + id);
+                    const T rtx = jst_shfl_down(nxr, 1), rty = jst_shfl_down(nyr, 1);
+                    const T iv = (T)ld(I.inv_vol + id);
+                    T g[8];
+                    for (int q = 0; q < 4; ++q) {
+                        const T cq = qw[1][q];
+                        const T lf = jst_shfl_up(cq, 1), rg = jst_shfl_down(cq, 1);
+                        if (sizeof(T) == sizeof(double))
+                            green_gauss<T>(cq, qk[q], qw[0][q], lf, rg, txk, tyk, tx[2], ty[2], nxr, nyr, rtx, rty, iv,
+                                           &g[2 * q], &g[2 * q + 1]);
+                        else
+                            green_gauss_delta<T>(cq, qk[q], qw[0][q], lf, rg, txk, tyk, tx[2], ty[2], nxr, nyr, rtx,
+                                                 rty, iv, &g[2 * q], &g[2 * q + 1]);
+                    }
+                    Diff<T> d = diffusion_tensor<T>(qw[1][2], u[3][4], qw[1][0], qw[1][1], g[0], g[1], g[2], g[3], g[4],
+                                                    g[5], g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num, (T)c.t_suth,
+                                                    (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp, (T)c.sigma);
+                    dn[0] = d.dx1;
+                    dn[1] = d.dx2;
+                    dn[2] = d.dx3;
+                    dn[3] = d.dx4;
+                    dn[4] = d.dy1;
+                    dn[5] = d.dy2;
+                    dn[6] = d.dy3;
+                    dn[7] = d.dy4;
+                    if (r >= i0 && r < i1) {
+                        T s5 = sa_source<T>(u[3][0], u[3][4], (T)ld(I.inv_d2 + id), d.chi, d.fv1, g[2], g[1], g[6],
+                                            g[7], c);
+                        snew = s5 * (T)ld(I.vol + id);
+                    }
+                    if (r == 0) {
+                        // the wall ghost ring (row -1, one row up in the window) takes cell
+                        // 0's gradient with grad T = 0 (gradient.rs:93-95)
+                        Diff<T> w = diffusion_tensor<T>(qw[0][2], u[2][4], qw[0][0], qw[0][1], g[0], g[1], g[2], g[3],
+                                                        T(0), T(0), g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num,
+                                                        (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt,
+                                                        (T)c.cp, (T)c.sigma);
+                        dw[1][0] = w.dx1;
+                        dw[1][1] = w.dx2;
+                        dw[1][2] = w.dx3;
+                        dw[1][3] = w.dx4;
+                        dw[1][4] = w.dy1;
+                        dw[1][5] = w.dy2;
+                        dw[1][6] = w.dy3;
+                        dw[1][7] = w.dy4;
+                    }
+                } else if (r >= ni) {  // far ghost ring: zero gradient (gradient.rs:96)
+                    Diff<T> d = diffusion_tensor<T>(qw[1][2], u[3][4], qw[1][0], qw[1][1], T(0), T(0), T(0), T(0),
+                                                    T(0), T(0), T(0), T(0), (T)c.inv_t_ref, (T)c.suth_num,
+                                                    (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp,
+                                                    (T)c.sigma);
+                    dn[0] = d.dx1;
+                    dn[1] = d.dx2;
+                    dn[2] = d.dx3;
+                    dn[3] = d.dx4;
+                    dn[4] = d.dy1;
+                    dn[5] = d.dy2;
+                    dn[6] = d.dy3;
+                    dn[7] = d.dy4;
+                }
+                // r == -1 on a wall strip: written when row 0 is reached
+            }
+
+            // ---- V/dt of row k-2 (clamped, dissipation.rs:59) --------------
+            T rtn = T(0);
+            {
+                int rr = k - 2;
+                int gc = rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr);
+                if (rr >= i0 - 1 && rr <= i1) rtn = ld(ratio + (long)gc * nj + gj);
+            }
+
+            // ---- tau face f = k-2 (between rows k-3 and k-2) ---------------
+            T ftn[5];
+            for (int v = 0; v < 5; ++v) ftn[v] = T(0);
+            const int f = k - 2;
+            if (f >= i0 && f <= i1) {
+                T m = tmax<T>(tmax<T>(tmax<T>(si[0], si[1]), si[2]), sik);
+                T e2 = k2 * m;
+                T e4 = tmax<T>(k4 - e2, T(0));
+                T lam = half_cfl * (rtn + rt0);
+                T fu[5], cv[5];
+                for (int v = 0; v < 5; ++v) fu[v] = T(0.5) * (u[1][v] + u[2][v]);
+                const T fnx = tx[1], fny = ty[1];
+                euler_flux<T>(fu, fnx, fny, gm1, cv, p_ref);
+                T hx = T(0.5) * fnx, hy = T(0.5) * fny;
+                for (int v = 0; v < 5; ++v) {
+                    T d1 = u[2][v] - u[1][v];
+                    T d3 = u[3][v] - T(3) * u[2][v] + T(3) * u[1][v] - u[0][v];
+                    T vis = T(0);
+                    if (v > 0) vis = (dw[0][v - 1] + dw[1][v - 1]) * hx + (dw[0][v + 3] + dw[1][v + 3]) * hy;
+                    ftn[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
+                }
+            }
+
+            // ---- n faces and the update of row m = k-3 ---------------------
+            const int m = k - 3;
+            if (m >= i0 && m < i1) {
+                // face between this lane's column and the one to its left
+                T fn[5];
+                {
+                    T m4 = tmax<T>(tmax<T>(tmax<T>(jst_shfl_up(sj[0], 2), jst_shfl_up(sj[0], 1)), sj[0]),
+                                   jst_shfl_down(sj[0], 1));
+                    T e2 = k2 * m4;
+                    T e4 = tmax<T>(k4 - e2, T(0));
+                    T lam = half_cfl * (rt0 + jst_shfl_up(rt0, 1));
+                    T ul1[5], ul2[5], ur1[5], fu[5], cv[5];
+                    for (int v = 0; v < 5; ++v) {
+                        ul1[v] = jst_shfl_up(u[1][v], 1);
+                        ul2[v] = jst_shfl_up(u[1][v], 2);
+                        ur1[v] = jst_shfl_down(u[1][v], 1);
+                        fu[v] = T(0.5) * (ul1[v] + u[1][v]);
+                    }
+                    euler_flux<T>(fu, nx2[0], ny2[0], gm1, cv, p_ref);
+                    T hx = T(0.5) * nx2[0], hy = T(0.5) * ny2[0];
+                    T dl[8];
+                    for (int v = 0; v < 8; ++v) dl[v] = jst_shfl_up(dw[0][v], 1);
+                    for (int v = 0; v < 5; ++v) {
+                        T d1 = u[1][v] - ul1[v];
+                        T d3 = ur1[v] - T(3) * u[1][v] + T(3) * ul1[v] - ul2[v];
+                        T vis = T(0);
+                        if (v > 0) vis = (dl[v - 1] + dw[0][v - 1]) * hx + (dl[v + 3] + dw[0][v + 3]) * hy;
+                        fn[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
+                    }
+                }
+                T fnr[5];
+                for (int v = 0; v < 5; ++v) fnr[v] = jst_shfl_down(fn[v], 1);
+                T nxr3 = T(0), nyr3 = T(0);
+                if (LAST) {
+                    nxr3 = jst_shfl_down(nx2[0], 1);
+                    nyr3 = jst_shfl_down(ny2[0], 1);
+                }
+                if (out_lane) {
+                    const long id = (long)m * nj + gj;
+                    T R[5];
+                    for (int v = 0; v < 5; ++v) R[v] = (ftn[v] - ft[v]) + (fnr[v] - fn[v]);
+                    R[4] -= sw[0];
+                    double a = alpha * (I.local_dt ? ld(I.ldt + id) : I.st->dt);
+                    double sc = a * ld(I.inv_vol + id);
+                    double un[5], uo0 = 0.0;
+                    for (int v = 0; v < 5; ++v) {
+                        double uo = I.un[v][id];
+                        if (v == 0) uo0 = uo;
+                        if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
+                        else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
+                        dst[v][id] = (TD)un[v];
+                        if (LAST && sizeof(T) != sizeof(double)) I.uc[v][id] = (T)un[v];
+                    }
+                    // unpack checks (solver.rs:160-171), on the stored precision
+                    bool bad;
+                    Prim<double> q{};
+                    if (sizeof(T) == sizeof(double)) {
+                        double rho = un[0];
+                        bad = isnan(rho) || rho <= 1e-15;
+                        if (!bad) {
+                            q = unpack_cell<double>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
+                            bad = isnan(q.p) || q.p <= 1e-15;
+                        }
+                    } else {
+                        T rho = (T)un[0];
+                        bad = isnan(rho) || rho <= T(1e-15);
+                        if (!bad) {
+                            Prim<T> qt = unpack_cell<T>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], gm1, rgas);
+                            bad = isnan(qt.p) || qt.p <= T(1e-15);
+                            q.vx = qt.vx;
+                            q.vy = qt.vy;
+                            q.t = qt.t;
+                        }
+                    }
+                    if (bad) {
+                        atomicMin(&I.st->bad, (stage_id << 32) | (unsigned long long)id);
+                    } else if (LAST) {
+                        double d = un[0] - uo0;  // solver.rs:195
+                        sres += d * d;
+                        // timestep.rs:30-42 in the stage arithmetic
+                        T aa = T(0.5) * (tx[0] + tx[1]);
+                        T bb = T(0.5) * (ty[0] + ty[1]);
+                        T cc = T(0.5) * (nx2[0] + nxr3);
+                        T dd = T(0.5) * (ny2[0] + nyr3);
+                        T vol = (T)ld(I.vol + id);
+                        T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
+                        T dl = local_dt<T>(qvx, qvy, sqrt((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
+                        ratio_next[id] = vol / dl;
+                        if (I.local_dt) I.ldt[id] = (double)dl;
+                        mloc = fmin(mloc, (double)dl);
+                    }
+                }
+            }
+
+            // ---- slide the windows ------------------------------------------
+            for (int v = 0; v < 5; ++v) {
+                u[0][v] = u[1][v];
+                u[1][v] = u[2][v];
+                u[2][v] = u[3][v];
+                u[3][v] = uk[v];
+                ft[v] = ftn[v];
+            }
+            nu3 = qw[0][3];
+            pw[0] = pw[1];
+            pw[1] = pk;
+            for (int v = 0; v < 4; ++v) {
+                qw[0][v] = qw[1][v];
+                qw[1][v] = qk[v];
+            }
+            si[0] = si[1];
+            si[1] = si[2];
+            si[2] = sik;
+            sj[0] = sj[1];
+            sj[1] = sj[2];
+            sj[2] = sjk;
+            for (int v = 0; v < 8; ++v) {
+                dw[0][v] = dw[1][v];
+                dw[1][v] = dn[v];
+            }
+            sw[0] = sw[1];
+            sw[1] = snew;
+            rt0 = rtn;
+            tx[0] = tx[1];
+            tx[1] = tx[2];
+            tx[2] = txk;
+            ty[0] = ty[1];
+            ty[1] = ty[2];
+            ty[2] = tyk;
+            nx2[0] = nx2[1];
+            nx2[1] = nxr;
+            ny2[0] = ny2[1];
+            ny2[1] = nyr;
+        }
+
+        if (LAST) {
+            double mn = warp_min(mloc);
+            double sr = warp_sum0(sres);
+            unsigned last = 0;
+            if (lane == 0) {
+                I.partial[2 * tr.tile] = mn;
+                I.partial[2 * tr.tile + 1] = sr;
+                JST_FENCE();
+                unsigned prev = atomicAdd(&I.st->counter, 1u);
+                last = prev == (unsigned)(I.ntiles - 1);
+            }
+            last = jst_shfl_idx(last, 0);
+            if (last) {
+                JST_FENCE();
+                finish_step_warp<T>(I, true);
+            }
+        }
+    }
+}
+
+}  // namespace fused
+}  // namespace jst

@@ -78,12 +78,14 @@ def test_fused_tile_shape_invariance_bitwise(tile):
         assert np.array_equal(a.get(f"U{k}"), b.get(f"U{k}")), k
 
 
-@pytest.mark.parametrize("cfgt", [(4, 32, 256), (8, 32, 128), (8, 32, 192), (16, 32, 384), (8, 64, 256)],
+@pytest.mark.parametrize("cfgt", [(4, 32, 256), (8, 32, 128), (8, 32, 192), (16, 32, 384), (8, 64, 256),
+                                  (16, 26, 128), (32, 26, 128), (64, 26, 128), (32, 26, 256), (32, 26, 64)],
                          ids=lambda t: "x".join(map(str, t)))
 def test_fused_every_compiled_configuration_matches_oracle(cfgt):
     """Every tile shape and block size the autotuner may pick (block sizes
-    that are not powers of two included) reproduces the oracle's residual
-    history, global time step and fields."""
+    that are not powers of two included, and the marching strips of 26
+    columns) reproduces the oracle's residual history, global time step and
+    fields."""
     cfg, xy, nr, nt = cylinder_case(33, 64)
     s = _solver(cfg, xy, nr, nt, tile_i=cfgt[0], tile_j=cfgt[1], block_threads=cfgt[2])
     o = jo.OracleSolver(cfg, xy, nr, nt)
