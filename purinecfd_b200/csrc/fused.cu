@@ -170,12 +170,13 @@ template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
 }
 
 template <class T, int H, int NT> Kernels<T> march_kernels_for() {
+    constexpr bool PIPE = true;
     Kernels<T> k;
-    k.stage[0] = fused::k_march<T, H, NT, true, false>;
-    k.stage[1] = fused::k_march<T, H, NT, false, false>;
-    k.stage[2] = fused::k_march<T, H, NT, false, true>;
+    k.stage[0] = fused::k_march<T, H, NT, true, false, PIPE>;
+    k.stage[1] = fused::k_march<T, H, NT, false, false, PIPE>;
+    k.stage[2] = fused::k_march<T, H, NT, false, true, PIPE>;
     k.step_dt = fused::k_step_dt<T, NT>;
-    k.smem = 0;
+    k.smem = fused::march_smem_bytes<T, NT, PIPE>();
     k.nt = NT;
     k.march = true;
     return k;

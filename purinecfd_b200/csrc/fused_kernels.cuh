@@ -307,6 +307,19 @@ template <int BYTES> JST_D void async_copy(void* dst, const void* src) {
 #endif
 }
 
+JST_D void async_commit() {
+#ifdef __CUDA_ARCH__
+    __pipeline_commit();
+#endif
+}
+
+// Wait until at most the most recently committed group is still in flight.
+JST_D void async_wait_prior1() {
+#ifdef __CUDA_ARCH__
+    __pipeline_wait_prior(1);
+#endif
+}
+
 JST_D void async_wait_all() {
 #ifdef __CUDA_ARCH__
     __pipeline_commit();

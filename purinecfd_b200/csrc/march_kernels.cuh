@@ -73,13 +73,45 @@ template <class T> JST_D void finish_step_warp(const Inst<T>& I, bool with_resid
     }
 }
 
+// One row's worth of global inputs of a warp, staged asynchronously one row
+// ahead (PIPE variant): [field][lane].
+template <class T> struct MarchRow {
+    double tx[32], ty[32];            // tau normals of face row k
+    double nx[32], ny[32], iv[32];    // n normals, 1/V of row k-1
+    double d2[32], vol[32];           // 1/d^2, V of row k-1
+    double un[5][32], ldt[32], ivm[32], volm[32];  // U_n, dt_local, 1/V, V of row k-3
+    T u[5][32];                       // stage input of row k
+    T rat[32];                        // V/dt of row k-2 (clamped)
+};
+
+template <class T, int NT, bool PIPE> constexpr size_t march_smem_bytes() {
+    return PIPE ? (size_t)(NT / 32) * 2 * sizeof(MarchRow<T>) : 0;
+}
+
+// Minimum resident blocks per SM asked of the register allocator: 12 warps
+// per SM in FP32 (at most 168 registers a thread; the last stage would take
+// ~190 and drop to 8 warps), no cap in FP64.  Measured on B200: the cap
+// takes the FP32 last stage from 0.48 to 0.35 ms on 4.2 M cells, and a
+// 16-warp cap (128 registers) spills and is slower.
+template <class T, int NT> constexpr int march_min_blocks() {
+    return sizeof(T) == sizeof(float) ? (12 / (NT / 32) > 0 ? 12 / (NT / 32) : 1) : 1;
+}
+
 // sched[0] = number of strips, sched[1] = work counter, sched[2] = exit counter
 // (both zero at launch; the last warp to leave resets them).
-template <class T, int H, int NT, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage,
+// PIPE: every global input of row k+1 is copied into a per-warp shared
+// buffer (cp.async) while row k is computed, so the walk never waits on HBM
+// latency; without PIPE the loads are issued in the row that uses them.
+template <class T, int H, int NT, bool FIRST, bool LAST, bool PIPE = false>
+__global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage,
                                               double alpha) {
     using TD = typename std::conditional<LAST, double, T>::type;
     const int lane = JST_LANE();
+    MarchRow<T>* rowbuf = nullptr;
+    if constexpr (PIPE) {
+        JST_DYN_SMEM(smem_raw);
+        rowbuf = reinterpret_cast<MarchRow<T>*>(smem_raw) + 2 * JST_WARP_IN_BLOCK();
+    }
     const int nt_all = sched[0];
     unsigned* work = reinterpret_cast<unsigned*>(sched + 1);
     unsigned* exitc = reinterpret_cast<unsigned*>(sched + 2);
@@ -137,6 +169,49 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
         const T half_cfl = (T)c.half_cfl, k2 = (T)c.k2, k4 = (T)c.k4;
         const T p_ref = sizeof(T) == sizeof(double) ? T(0) : (T)c.p_inf;  // see euler_flux
 
+        // PIPE: stage the global inputs that row kk of the walk reads.  The
+        // conditions are the ones under which the walk reads them.
+        auto issue = [&](int kk) {
+            MarchRow<T>& B = rowbuf[kk & 1];
+            if (kk < ni) {
+                const long id = (long)(kk < 0 ? -1 - kk : kk) * nj + gj;
+                for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.u[v][lane], src[v] + id);
+            }
+            if (kk >= 0 && kk <= ni) {
+                const long f = (long)kk * nj + gj;
+                async_copy<8>(&B.tx[lane], I.tnx + f);
+                async_copy<8>(&B.ty[lane], I.tny + f);
+            }
+            const int r = kk - 1;
+            if (r >= i0 - 1 && r <= i1 && r >= 0 && r < ni) {
+                const long id = (long)r * nj + gj;
+                async_copy<8>(&B.nx[lane], I.nnx + id);
+                async_copy<8>(&B.ny[lane], I.nny + id);
+                async_copy<8>(&B.iv[lane], I.inv_vol + id);
+                if (r >= i0 && r < i1) {
+                    async_copy<8>(&B.d2[lane], I.inv_d2 + id);
+                    async_copy<8>(&B.vol[lane], I.vol + id);
+                }
+            }
+            const int rr = kk - 2;
+            if (rr >= i0 - 1 && rr <= i1) {
+                const int gc = rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr);
+                async_copy<sizeof(T)>(&B.rat[lane], ratio + (long)gc * nj + gj);
+            }
+            const int m = kk - 3;
+            if (m >= i0 && m < i1) {
+                const long id = (long)m * nj + gj;
+                for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[v] + id);
+                if (I.local_dt) async_copy<8>(&B.ldt[lane], I.ldt + id);
+                async_copy<8>(&B.ivm[lane], I.inv_vol + id);
+                if (LAST) async_copy<8>(&B.volm[lane], I.vol + id);
+            }
+        };
+        if constexpr (PIPE) {
+            issue(i0 - 3);
+            async_commit();
+        }
+
         // sliding windows (index 0 = oldest row)
         T u[4][5];      // U rows k-4 .. k-1
         T pw[2];        // p rows k-2, k-1
@@ -168,13 +243,20 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
         double sres = 0.0;
 
         for (int k = i0 - 3; k <= i1 + 2; ++k) {
+            const MarchRow<T>* B = nullptr;
+            if constexpr (PIPE) {
+                if (k + 1 <= i1 + 2) issue(k + 1);
+                async_commit();
+                async_wait_prior1();
+                B = &rowbuf[k & 1];
+            }
             // ---- row k: conserved state and primitives ---------------------
             T uk[5], pk, qk[4];
             if (k < ni) {
                 const bool wall = k < 0;
                 const int kr = wall ? -1 - k : k;  // the wall ghost mirrors cell -1-k (boundary.rs:30-51)
                 const long id = (long)kr * nj + gj;
-                for (int v = 0; v < 5; ++v) uk[v] = ld(src[v] + id);
+                for (int v = 0; v < 5; ++v) uk[v] = PIPE ? B->u[v][lane] : ld(src[v] + id);
                 Prim<T> p;
                 if (fresh) {
                     p.rho = (T)c.f_rho;
@@ -240,8 +322,8 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
             T txk = T(0), tyk = T(0);
             if (k >= 0 && k <= ni) {
                 long f = (long)k * nj + gj;
-                txk = (T)ld(I.tnx + f);
-                tyk = (T)ld(I.tny + f);
+                txk = (T)(PIPE ? B->tx[lane] : ld(I.tnx + f));
+                tyk = (T)(PIPE ? B->ty[lane] : ld(I.tny + f));
             }
 
             // ---- gradients, diffusion tensor, SA source of row r = k-1 -----
@@ -252,10 +334,10 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
             if (r >= i0 - 1 && r <= i1) {
                 if (r >= 0 && r < ni) {
                     const long id = (long)r * nj + gj;
-                    nxr = (T)ld(I.nnx + id);
-                    nyr = (T)ld(I.nny + id);
+                    nxr = (T)(PIPE ? B->nx[lane] : ld(I.nnx + id));
+                    nyr = (T)(PIPE ? B->ny[lane] : ld(I.nny + id));
                     const T rtx = jst_shfl_down(nxr, 1), rty = jst_shfl_down(nyr, 1);
-                    const T iv = (T)ld(I.inv_vol + id);
+                    const T iv = (T)(PIPE ? B->iv[lane] : ld(I.inv_vol + id));
                     T g[8];
                     for (int q = 0; q < 4; ++q) {
                         const T cq = qw[1][q];
@@ -279,9 +361,9 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
                     dn[6] = d.dy3;
                     dn[7] = d.dy4;
                     if (r >= i0 && r < i1) {
-                        T s5 = sa_source<T>(u[3][0], u[3][4], (T)ld(I.inv_d2 + id), d.chi, d.fv1, g[2], g[1], g[6],
-                                            g[7], c);
-                        snew = s5 * (T)ld(I.vol + id);
+                        T s5 = sa_source<T>(u[3][0], u[3][4], (T)(PIPE ? B->d2[lane] : ld(I.inv_d2 + id)), d.chi,
+                                            d.fv1, g[2], g[1], g[6], g[7], c);
+                        snew = s5 * (T)(PIPE ? B->vol[lane] : ld(I.vol + id));
                     }
                     if (r == 0) {
                         // the wall ghost ring (row -1, one row up in the window) takes cell
@@ -321,7 +403,7 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
             {
                 int rr = k - 2;
                 int gc = rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr);
-                if (rr >= i0 - 1 && rr <= i1) rtn = ld(ratio + (long)gc * nj + gj);
+                if (rr >= i0 - 1 && rr <= i1) rtn = PIPE ? B->rat[lane] : ld(ratio + (long)gc * nj + gj);
             }
 
             // ---- tau face f = k-2 (between rows k-3 and k-2) ---------------
@@ -389,11 +471,11 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
                     T R[5];
                     for (int v = 0; v < 5; ++v) R[v] = (ftn[v] - ft[v]) + (fnr[v] - fn[v]);
                     R[4] -= sw[0];
-                    double a = alpha * (I.local_dt ? ld(I.ldt + id) : I.st->dt);
-                    double sc = a * ld(I.inv_vol + id);
+                    double a = alpha * (I.local_dt ? (PIPE ? B->ldt[lane] : ld(I.ldt + id)) : I.st->dt);
+                    double sc = a * (PIPE ? B->ivm[lane] : ld(I.inv_vol + id));
                     double un[5], uo0 = 0.0;
                     for (int v = 0; v < 5; ++v) {
-                        double uo = I.un[v][id];
+                        double uo = PIPE ? B->un[v][lane] : I.un[v][id];
                         if (v == 0) uo0 = uo;
                         if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
                         else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
@@ -431,7 +513,7 @@ __global__ void __launch_bounds__(NT) k_march(const TileRef* tiles, int* sched, 
                         T bb = T(0.5) * (ty[0] + ty[1]);
                         T cc = T(0.5) * (nx2[0] + nxr3);
                         T dd = T(0.5) * (ny2[0] + nyr3);
-                        T vol = (T)ld(I.vol + id);
+                        T vol = (T)(PIPE ? B->volm[lane] : ld(I.vol + id));
                         T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
                         T dl = local_dt<T>(qvx, qvy, sqrt((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
                         ratio_next[id] = vol / dl;
