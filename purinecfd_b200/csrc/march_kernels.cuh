@@ -171,35 +171,36 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
 
         // PIPE: stage the global inputs that row kk of the walk reads.  The
         // conditions are the ones under which the walk reads them.
-        auto issue = [&](int kk) {
+        auto issue = [&](auto steady, int kk) {
+            constexpr bool S = decltype(steady)::value;  // kk is a steady row
             MarchRow<T>& B = rowbuf[kk & 1];
-            if (kk < ni) {
+            if (S || kk < ni) {
                 const long id = (long)(kk < 0 ? -1 - kk : kk) * nj + gj;
                 for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.u[v][lane], src[v] + id);
             }
-            if (kk >= 0 && kk <= ni) {
+            if (S || (kk >= 0 && kk <= ni)) {
                 const long f = (long)kk * nj + gj;
                 async_copy<8>(&B.tx[lane], I.tnx + f);
                 async_copy<8>(&B.ty[lane], I.tny + f);
             }
             const int r = kk - 1;
-            if (r >= i0 - 1 && r <= i1 && r >= 0 && r < ni) {
+            if (S || (r >= i0 - 1 && r <= i1 && r >= 0 && r < ni)) {
                 const long id = (long)r * nj + gj;
                 async_copy<8>(&B.nx[lane], I.nnx + id);
                 async_copy<8>(&B.ny[lane], I.nny + id);
                 async_copy<8>(&B.iv[lane], I.inv_vol + id);
-                if (r >= i0 && r < i1) {
+                if (S || (r >= i0 && r < i1)) {
                     async_copy<8>(&B.d2[lane], I.inv_d2 + id);
                     async_copy<8>(&B.vol[lane], I.vol + id);
                 }
             }
             const int rr = kk - 2;
-            if (rr >= i0 - 1 && rr <= i1) {
-                const int gc = rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr);
+            if (S || (rr >= i0 - 1 && rr <= i1)) {
+                const int gc = S ? rr : (rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr));
                 async_copy<sizeof(T)>(&B.rat[lane], ratio + (long)gc * nj + gj);
             }
             const int m = kk - 3;
-            if (m >= i0 && m < i1) {
+            if (S || (m >= i0 && m < i1)) {
                 const long id = (long)m * nj + gj;
                 for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[v] + id);
                 if (I.local_dt) async_copy<8>(&B.ldt[lane], I.ldt + id);
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             }
         };
         if constexpr (PIPE) {
-            issue(i0 - 3);
+            issue(std::false_type{}, i0 - 3);
             async_commit();
         }
 
@@ -242,18 +243,23 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         double mloc = __longlong_as_double(0x7ff0000000000000LL);
         double sres = 0.0;
 
-        for (int k = i0 - 3; k <= i1 + 2; ++k) {
+        // One row of the walk.  S (steady): k in [i0+3, i1-2], where every
+        // phase is active, no ghost row is involved and the next row is steady
+        // too, so the range tests drop out and the body is one straight block.
+        auto row = [&](auto steady, int k) {
+            constexpr bool S = decltype(steady)::value;
             const MarchRow<T>* B = nullptr;
             if constexpr (PIPE) {
-                if (k + 1 <= i1 + 2) issue(k + 1);
+                if (S) issue(steady, k + 1);
+                else if (k + 1 <= i1 + 2) issue(std::false_type{}, k + 1);
                 async_commit();
                 async_wait_prior1();
                 B = &rowbuf[k & 1];
             }
             // ---- row k: conserved state and primitives ---------------------
             T uk[5], pk, qk[4];
-            if (k < ni) {
-                const bool wall = k < 0;
+            if (S || k < ni) {
+                const bool wall = !S && k < 0;
                 const int kr = wall ? -1 - k : k;  // the wall ghost mirrors cell -1-k (boundary.rs:30-51)
                 const long id = (long)kr * nj + gj;
                 for (int v = 0; v < 5; ++v) uk[v] = PIPE ? B->u[v][lane] : ld(src[v] + id);
@@ -320,7 +326,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
 
             // ---- tau normals of face row k ---------------------------------
             T txk = T(0), tyk = T(0);
-            if (k >= 0 && k <= ni) {
+            if (S || (k >= 0 && k <= ni)) {
                 long f = (long)k * nj + gj;
                 txk = (T)(PIPE ? B->tx[lane] : ld(I.tnx + f));
                 tyk = (T)(PIPE ? B->ty[lane] : ld(I.tny + f));
@@ -331,8 +337,8 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             T dn[8];
             for (int v = 0; v < 8; ++v) dn[v] = T(0);
             T snew = T(0), nxr = T(0), nyr = T(0);
-            if (r >= i0 - 1 && r <= i1) {
-                if (r >= 0 && r < ni) {
+            if (S || (r >= i0 - 1 && r <= i1)) {
+                if (S || (r >= 0 && r < ni)) {
                     const long id = (long)r * nj + gj;
                     nxr = (T)(PIPE ? B->nx[lane] : ld(I.nnx + id));
                     nyr = (T)(PIPE ? B->ny[lane] : ld(I.nny + id));
@@ -360,12 +366,12 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     dn[5] = d.dy2;
                     dn[6] = d.dy3;
                     dn[7] = d.dy4;
-                    if (r >= i0 && r < i1) {
+                    if (S || (r >= i0 && r < i1)) {
                         T s5 = sa_source<T>(u[3][0], u[3][4], (T)(PIPE ? B->d2[lane] : ld(I.inv_d2 + id)), d.chi,
                                             d.fv1, g[2], g[1], g[6], g[7], c);
                         snew = s5 * (T)(PIPE ? B->vol[lane] : ld(I.vol + id));
                     }
-                    if (r == 0) {
+                    if (!S && r == 0) {
                         // the wall ghost ring (row -1, one row up in the window) takes cell
                         // 0's gradient with grad T = 0 (gradient.rs:93-95)
                         Diff<T> w = diffusion_tensor<T>(qw[0][2], u[2][4], qw[0][0], qw[0][1], g[0], g[1], g[2], g[3],
@@ -402,15 +408,15 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             T rtn = T(0);
             {
                 int rr = k - 2;
-                int gc = rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr);
-                if (rr >= i0 - 1 && rr <= i1) rtn = PIPE ? B->rat[lane] : ld(ratio + (long)gc * nj + gj);
+                int gc = S ? rr : (rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr));
+                if (S || (rr >= i0 - 1 && rr <= i1)) rtn = PIPE ? B->rat[lane] : ld(ratio + (long)gc * nj + gj);
             }
 
             // ---- tau face f = k-2 (between rows k-3 and k-2) ---------------
             T ftn[5];
             for (int v = 0; v < 5; ++v) ftn[v] = T(0);
             const int f = k - 2;
-            if (f >= i0 && f <= i1) {
+            if (S || (f >= i0 && f <= i1)) {
                 T m = tmax<T>(tmax<T>(tmax<T>(si[0], si[1]), si[2]), sik);
                 T e2 = k2 * m;
                 T e4 = tmax<T>(k4 - e2, T(0));
@@ -431,7 +437,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
 
             // ---- n faces and the update of row m = k-3 ---------------------
             const int m = k - 3;
-            if (m >= i0 && m < i1) {
+            if (S || (m >= i0 && m < i1)) {
                 // face between this lane's column and the one to its left
                 T fn[5];
                 {
@@ -561,7 +567,12 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             nx2[1] = nxr;
             ny2[0] = ny2[1];
             ny2[1] = nyr;
-        }
+        };
+        const int ks0 = i0 + 3, ks1 = i1 - 2;  // steady rows
+        int k = i0 - 3;
+        for (; k < ks0 && k <= i1 + 2; ++k) row(std::false_type{}, k);
+        for (; k <= ks1; ++k) row(std::true_type{}, k);
+        for (; k <= i1 + 2; ++k) row(std::false_type{}, k);
 
         if (LAST) {
             double mn = warp_min(mloc);
