@@ -38,20 +38,34 @@ sys.path.insert(0, str(ROOT))
 METRIC = "solves/s & p99 at CL/CD err<=1e-4, batched FP32 vs plain FP64; Mcell-stage/s"
 UNIT = "Mcell-stage/s"
 
-# Algorithmic (compulsory) HBM bytes per cell per stage of the fused kernels,
-# averaged over the 5 stages of a step (geometry: tau and n normals 32 B,
-# vol 8, 1/V 8, 1/d^2 8 = 56 B; U_n FP64 40 B; stage state T; ratio T):
-#   FP64:  stage 1: U_n 40 + write 40 + geom 56 + ratio 8                 = 144
-#          stages 2-4: U 40 + U_n 40 + write 40 + geom 56 + ratio 8       = 184
-#          stage 5: U 40 + U_n 40 + write U_n 40 + geom 56 + ratio 8+8    = 192
-#          average 177.6 B
-#   split (stage 1 reads the FP32 copy of U_n that stage 5 writes):
-#          stages 1-4: U 20 + U_n 40 + write 20 + geom 56 + ratio 4       = 140
-#          stage 5: U 20 + U_n 40 + write U_n 40 + FP32 copy 20 + geom 56
-#                   + ratio 4+4                                           = 184
-#          average 148.8 B
-BYTES_PER_CELL_STAGE = {"fp64": (144 + 3 * 184 + 192) / 5.0, "split": (4 * 140 + 184) / 5.0}
-BYTES_PER_STAGE = {"fp64": [144, 184, 184, 184, 192], "split": [140, 140, 140, 140, 184]}
+# Algorithmic (compulsory) HBM bytes per cell per stage of the stage kernels
+# (U_n FP64 40 B; stage state and V/dt in the stage type T).
+# Marching kernel (the autotuner's choice on large meshes): geometry is one
+# record of 8 T per cell (tau and n normals, 1/V, 1/d^2, V, pad) plus the
+# FP64 1/V of the updated cell (8 B):
+#   split: stages 1-4: U 20 + U_n 40 + write 20 + record 32 + 1/V 8 + ratio 4       = 124
+#          stage 5: U 20 + U_n 40 + write U_n 40 + FP32 copy 20 + record 32 + 1/V 8
+#                   + V 4 + ratio 4+4                                               = 172
+#          average 133.6 B
+#   FP64:  stage 1: U_n 40 + write 40 + record 64 + 1/V 8 + ratio 8                 = 160
+#          stages 2-4: U 40 + U_n 40 + write 40 + record 64 + 1/V 8 + ratio 8       = 200
+#          stage 5: U 40 + U_n 40 + write U_n 40 + record 64 + 1/V 8 + V 8
+#                   + ratio 8+8                                                     = 216
+#          average 195.2 B
+# Tile kernel: geometry = tau and n normals 32 B, V 8, 1/V 8, 1/d^2 8 = 56 B (FP64):
+#   split: stages 1-4: U 20 + U_n 40 + write 20 + geom 56 + ratio 4  = 140;  stage 5: 184;  average 148.8 B
+#   FP64:  stage 1: 144;  stages 2-4: 184;  stage 5: 192;  average 177.6 B
+BYTES_PER_STAGE = {("march", "split"): [124, 124, 124, 124, 172], ("march", "fp64"): [160, 200, 200, 200, 216],
+                   ("tile", "split"): [140, 140, 140, 140, 184], ("tile", "fp64"): [144, 184, 184, 184, 192]}
+
+
+def kernel_kind(kcfg) -> str:
+    """(tile_i, tile_j, threads) -> which stage kernel runs (strips are 26 wide)."""
+    return "march" if kcfg[1] == 26 else "tile"
+
+
+def bytes_per_cell_stage(kind: str, prec: str) -> float:
+    return sum(BYTES_PER_STAGE[(kind, prec)]) / 5.0
 
 
 def measured_peaks():
@@ -62,10 +76,10 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(prec: str):
+def ncu_traffic(kind: str, prec: str):
     """DRAM bytes per cell-stage of the stage kernel from the committed ncu
-    summary (profiles/stage_kernel_*.md, line `traffic_bytes_per_cell_stage <prec> <value>`)."""
-    for f in sorted((ROOT / "profiles").glob("*.md")):
+    summary (profiles/<kind>_kernel_*.md, line `traffic_bytes_per_cell_stage <prec> <value>`)."""
+    for f in sorted((ROOT / "profiles").glob(f"{kind}_kernel_*.md")):
         for line in f.read_text().splitlines():
             parts = line.strip().strip("`").split()
             if len(parts) == 3 and parts[0] == "traffic_bytes_per_cell_stage" and parts[1] == prec:
@@ -255,7 +269,8 @@ def run_ours(args, world, rank, local):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if args.precision == "split" else "f64", "data": "synthetic",
             "config": {"workload": args.workload, "cells": cells, "precision": args.precision,
-                       "path": "fused tiled stage kernel, CUDA graph per RK step",
+                       "path": ("warp-marching strip" if kernel_kind(kcfg) == "march" else "tiled") +
+                               " stage kernel, one launch per RK stage, CUDA graph per RK step",
                        "tile": "x".join(map(str, kcfg)) + (" (autotuned)" if not args.tile else ""),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (state + geometry ~0.7 GB)"},
@@ -263,14 +278,16 @@ def run_ours(args, world, rank, local):
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        bps = BYTES_PER_CELL_STAGE[args.precision]
+        kind = kernel_kind(kcfg)
+        bps = bytes_per_cell_stage(kind, args.precision)
         stage_avg = sum(stage_ms) / 5.0
         achieved = bps * cells / (stage_avg / 1e3) / 1e9
-        trafc = ncu_traffic(args.precision)
+        trafc = ncu_traffic(kind, args.precision)
         line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                             "traffic": None if trafc is None else round(trafc * cells),
-                            "kernel": "k_stage (5 launches per step; stage times " +
+                            "kernel": ("k_march" if kind == "march" else "k_stage") +
+                                      " (5 launches per step; stage times " +
                                       ", ".join(f"{x:.3f}" for x in stage_ms) + " ms)",
                             "bytes_per_cell_stage": round(bps, 1)}
         line["clocks"] = clk.summary()
@@ -280,12 +297,14 @@ def run_ours(args, world, rank, local):
             k64 = max(5, min(args.steps, 100))
             ms64, st64 = s64.time_steps(k64, stages=True)
             v64 = cells * 5 * k64 / (ms64 / 1e3) / 1e6
-            a64 = BYTES_PER_CELL_STAGE["fp64"] * cells / (sum(st64) / 5.0 / 1e3) / 1e9
+            b64 = bytes_per_cell_stage(kernel_kind(s64.kernel_config()), "fp64")
+            a64 = b64 * cells / (sum(st64) / 5.0 / 1e3) / 1e9
             line["fp64_plain"] = {"value": round(v64, 3), "unit": UNIT, "steps": k64,
                                   "ms_per_step": round(ms64 / k64, 5),
                                   "roofline": {"achieved": round(a64, 1), "peak": peak, "unit": "GB/s",
                                                "frac": round(a64 / peak, 4),
-                                               "bytes_per_cell_stage": BYTES_PER_CELL_STAGE["fp64"]}}
+                                               "bytes_per_cell_stage": b64,
+                                               "kernel": "x".join(map(str, s64.kernel_config()))}}
             s64.close()
         # end to end through the public API from host buffers: create (mesh H2D,
         # geometry on the GPU), K steps with the per-step residual read back,

@@ -200,6 +200,12 @@ template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 2
     return false;
 }
 
+template <class T> void build_march_geom(const Geom& g, int ni, int nj, T* rec, cudaStream_t st) {
+    long n = (long)(ni + 1) * nj;
+    JST_LAUNCH(fused::k_march_geom<T>, (unsigned)((n + 255) / 256), 256, 0, st, g.tnx, g.tny, g.nnx, g.nny, g.inv_vol,
+               g.inv_d2, g.vol, ni, nj, rec);
+}
+
 // Grid of a stage launch over `items` work items: one block per tile for the
 // tile kernels; for the marching kernels enough blocks to give every strip a
 // warp, at most the resident limit (warps take strips from a work counter).
@@ -320,6 +326,33 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
 
 }  // namespace
 
+// One primitive field of U_n (Solver::unpack, solver.rs:158-181) on the
+// device, so that a field read copies one plane instead of five.  The _rn
+// intrinsics keep the reference's separate roundings (no FMA contraction).
+__global__ void k_prim_field(UnPtrs un, long n, int id, PhysConst c, double* out) {
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    double rho = un.u[0][q], inv = 1.0 / rho;
+    double vx = __dmul_rn(un.u[1][q], inv), vy = __dmul_rn(un.u[2][q], inv);
+    double e = __dmul_rn(un.u[3][q], inv);
+    double ke = __dmul_rn(__dmul_rn(rho, __dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy))), 0.5);
+    double p = __dmul_rn(c.gm1, __dsub_rn(un.u[3][q], ke));
+    double t = p / __dmul_rn(c.r_gas, rho);
+    double v;
+    switch (id) {
+        case JST_F_RHO: v = rho; break;
+        case JST_F_P: v = p; break;
+        case JST_F_T: v = t; break;
+        case JST_F_U: v = vx; break;
+        case JST_F_V: v = vy; break;
+        case JST_F_E: v = e; break;
+        case JST_F_H: v = __dadd_rn(e, __dmul_rn(p, inv)); break;
+        case JST_F_C: v = sqrt(__dmul_rn(c.rg, t)); break;
+        default: v = __dmul_rn(un.u[4][q], inv); break;
+    }
+    out[q] = v;
+}
+
 template <class T> class FusedEngine : public Engine {
   public:
     explicit FusedEngine(SolverCore* core) : core_(core) {}
@@ -391,6 +424,8 @@ template <class T> class FusedEngine : public Engine {
         size_t o_unptr = add(5 * sizeof(double*));
         hist_cap_ = 4096;
         size_t o_hist = add(hist_cap_ * sizeof(double));
+        size_t o_field = add(n * sizeof(double));
+        size_t o_mg = add((size_t)(ni + 1) * nj * fused::MG_N * sizeof(T));
         if (cudaMalloc(&arena_, bytes) != cudaSuccess) {
             err = "cudaMalloc failed for the fused-path state (" + std::to_string(bytes >> 20) + " MiB)";
             return false;
@@ -429,6 +464,8 @@ template <class T> class FusedEngine : public Engine {
         d_force_ = reinterpret_cast<double*>(base + o_force);
         d_ntiles_ = reinterpret_cast<int*>(base + o_ntiles);
         d_unptr_ = reinterpret_cast<double**>(base + o_unptr);
+        d_field_ = reinterpret_cast<double*>(base + o_field);
+        inst_.mg = reinterpret_cast<T*>(base + o_mg);
         cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_ntiles_, &ntiles_, sizeof(int), cudaMemcpyHostToDevice, C.st);
@@ -438,6 +475,7 @@ template <class T> class FusedEngine : public Engine {
             return false;
         }
         JST_LAUNCH(k_far_geom, (nj + 255) / 256, 256, 0, C.st, C.g, const_cast<double*>(inst_.far));
+        build_march_geom(C.g, ni, nj, const_cast<T*>(inst_.mg), C.st);
         return cudaGetLastError() == cudaSuccess;
     }
 
@@ -672,32 +710,11 @@ template <class T> class FusedEngine : public Engine {
             std::fill(out, out + n, v[id]);
             return true;
         }
-        std::vector<double> u(5 * n);
-        for (int k = 0; k < 5; ++k)
-            if (cudaMemcpy(u.data() + k * n, inst_.un[k], n * sizeof(double), cudaMemcpyDeviceToHost) !=
-                cudaSuccess)
-                return false;
-        for (size_t q = 0; q < n; ++q) {
-            // solver.rs:158-181
-            double rho = u[q], inv = 1.0 / rho;
-            double vx = u[n + q] * inv, vy = u[2 * n + q] * inv, e = u[3 * n + q] * inv;
-            double p = c.gm1 * (u[3 * n + q] - rho * (vx * vx + vy * vy) * 0.5);
-            double t = p / (c.r_gas * rho);
-            double v;
-            switch (id) {
-                case JST_F_RHO: v = rho; break;
-                case JST_F_P: v = p; break;
-                case JST_F_T: v = t; break;
-                case JST_F_U: v = vx; break;
-                case JST_F_V: v = vy; break;
-                case JST_F_E: v = e; break;
-                case JST_F_H: v = e + p * inv; break;
-                case JST_F_C: v = std::sqrt(c.rg * t); break;
-                default: v = u[4 * n + q] * inv; break;
-            }
-            out[q] = v;
-        }
-        return true;
+        UnPtrs up;
+        for (int k = 0; k < 5; ++k) up.u[k] = inst_.un[k];
+        JST_LAUNCH(k_prim_field, (unsigned)((n + 255) / 256), 256, 0, core_->st, up, (long)n, id, c, d_field_);
+        return cudaMemcpyAsync(out, d_field_, n * sizeof(double), cudaMemcpyDeviceToHost, core_->st) == cudaSuccess &&
+               cudaStreamSynchronize(core_->st) == cudaSuccess;
     }
 
     jst_status set_conserved(const double* u5, jst_nonphysical* bad) override {
@@ -816,6 +833,7 @@ template <class T> class FusedEngine : public Engine {
     double* d_force_ = nullptr;
     int* d_ntiles_ = nullptr;
     double** d_unptr_ = nullptr;
+    double* d_field_ = nullptr;
     InstState* h_state_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
 };
@@ -1092,6 +1110,7 @@ template <class T> class Batch : public BatchBase {
         add(n * sizeof(double));                     // localdt
         add(2 * (size_t)ntiles * sizeof(double));    // partials
         add(5 * (size_t)nt * sizeof(double));        // far
+        add(ntau * fused::MG_N * sizeof(T));         // marching geometry records
         return b;
     }
 
@@ -1190,12 +1209,14 @@ template <class T> class Batch : public BatchBase {
             I.partial = reinterpret_cast<double*>(take(2 * (size_t)ptl * sizeof(double)));
             double* far = reinterpret_cast<double*>(take(5 * (size_t)nj * sizeof(double)));
             I.far = far;
+            I.mg = reinterpret_cast<T*>(take((size_t)(ni + 1) * nj * fused::MG_N * sizeof(T)));
             I.res_hist = nullptr;
             I.st = d_states_ + slot;
             I.c = c;
             cudaMemcpyAsync(d_xy, p.xy.data(), p.xy.size() * sizeof(double), cudaMemcpyHostToDevice, st_);
             geometry_build(d_xy, p.n_rings, nj, g, st_);
             JST_LAUNCH(k_far_geom, (nj + 255) / 256, 256, 0, st_, g, far);
+            build_march_geom(g, ni, nj, const_cast<T*>(I.mg), st_);
             JST_LAUNCH(k_fill_freestream, (unsigned)((n + 255) / 256), 256, 0, st_, I.un[0], I.un[1], I.un[2],
                        I.un[3], I.un[4], (long)n, c);
             InstState s0{};

@@ -85,6 +85,10 @@ template <class T> struct Inst {
     double* res_hist;   // residual per completed step (may be null)
     InstState* st;
     PhysConst c;
+    // marching kernels: per (row k in 0..NI, column j) the record
+    // {tau nx, ny of face row k; n nx, ny, 1/V, 1/d^2, V of cell row k-1; 0}
+    // in the stage type (zeros for cell row -1), see k_march_geom
+    const T* mg;
 };
 
 struct TileRef {

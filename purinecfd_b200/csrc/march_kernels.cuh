@@ -73,15 +73,45 @@ template <class T> JST_D void finish_step_warp(const Inst<T>& I, bool with_resid
     }
 }
 
+// Geometry record of row k (Inst::mg), 8 values of the stage type.
+enum { MG_TX = 0, MG_TY, MG_NX, MG_NY, MG_IV, MG_D2, MG_VOL, MG_N = 8 };
+
+// Builds Inst::mg from the FP64 geometry: the values each row of the walk
+// reads, rounded once to the stage type (the same values the stage
+// arithmetic used to convert at every use), in one 16-byte-aligned record.
+#ifdef __CUDACC__
+template <class T>
+__global__ void k_march_geom(const double* tnx, const double* tny, const double* nnx, const double* nny,
+                             const double* inv_vol, const double* inv_d2, const double* vol, int ni, int nj, T* rec) {
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long)(ni + 1) * nj) return;
+    T* r = rec + MG_N * q;
+    r[MG_TX] = (T)tnx[q];
+    r[MG_TY] = (T)tny[q];
+    if (q >= nj) {
+        long c = q - nj;
+        r[MG_NX] = (T)nnx[c];
+        r[MG_NY] = (T)nny[c];
+        r[MG_IV] = (T)inv_vol[c];
+        r[MG_D2] = (T)inv_d2[c];
+        r[MG_VOL] = (T)vol[c];
+    } else {
+        r[MG_NX] = r[MG_NY] = r[MG_IV] = r[MG_D2] = r[MG_VOL] = T(0);
+    }
+    r[7] = T(0);
+}
+#endif
+
 // One row's worth of global inputs of a warp, staged asynchronously one row
-// ahead (PIPE variant): [field][lane].
+// ahead (PIPE variant): [field][lane]; the geometry record in 16-byte chunks
+// [chunk][lane] so that each chunk read is one conflict-free 128-bit load.
 template <class T> struct MarchRow {
-    double tx[32], ty[32];            // tau normals of face row k
-    double nx[32], ny[32], iv[32];    // n normals, 1/V of row k-1
-    double d2[32], vol[32];           // 1/d^2, V of row k-1
-    double un[5][32], ldt[32], ivm[32], volm[32];  // U_n, dt_local, 1/V, V of row k-3
+    static constexpr int RCH = MG_N * (int)sizeof(T) / 16, EPC = 16 / (int)sizeof(T);
+    alignas(16) T rec[RCH][32][EPC];  // Inst::mg record of row k
+    double un[5][32], ldt[32], ivm[32];  // U_n, dt_local, 1/V of row k-3
     T u[5][32];                       // stage input of row k
     T rat[32];                        // V/dt of row k-2 (clamped)
+    T volm[32];                       // V of row k-3 (last stage)
 };
 
 template <class T, int NT, bool PIPE> constexpr size_t march_smem_bytes() {
@@ -179,20 +209,9 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.u[v][lane], src[v] + id);
             }
             if (S || (kk >= 0 && kk <= ni)) {
-                const long f = (long)kk * nj + gj;
-                async_copy<8>(&B.tx[lane], I.tnx + f);
-                async_copy<8>(&B.ty[lane], I.tny + f);
-            }
-            const int r = kk - 1;
-            if (S || (r >= i0 - 1 && r <= i1 && r >= 0 && r < ni)) {
-                const long id = (long)r * nj + gj;
-                async_copy<8>(&B.nx[lane], I.nnx + id);
-                async_copy<8>(&B.ny[lane], I.nny + id);
-                async_copy<8>(&B.iv[lane], I.inv_vol + id);
-                if (S || (r >= i0 && r < i1)) {
-                    async_copy<8>(&B.d2[lane], I.inv_d2 + id);
-                    async_copy<8>(&B.vol[lane], I.vol + id);
-                }
+                const T* g = I.mg + MG_N * ((long)kk * nj + gj);
+                for (int ch = 0; ch < MarchRow<T>::RCH; ++ch)
+                    async_copy<16>(&B.rec[ch][lane][0], g + ch * MarchRow<T>::EPC);
             }
             const int rr = kk - 2;
             if (S || (rr >= i0 - 1 && rr <= i1)) {
@@ -205,7 +224,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[v] + id);
                 if (I.local_dt) async_copy<8>(&B.ldt[lane], I.ldt + id);
                 async_copy<8>(&B.ivm[lane], I.inv_vol + id);
-                if (LAST) async_copy<8>(&B.volm[lane], I.vol + id);
+                if (LAST) async_copy<sizeof(T)>(&B.volm[lane], I.mg + MG_N * (id + nj) + MG_VOL);
             }
         };
         if constexpr (PIPE) {
@@ -324,13 +343,20 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             // i-sensor of row k-1
             const T sik = pressure_sensor<T>(pw[0], pw[1], pk);
 
-            // ---- tau normals of face row k ---------------------------------
-            T txk = T(0), tyk = T(0);
+            // ---- geometry record of row k (tau normals of face row k; n
+            // normals, 1/V, 1/d^2, V of cell row k-1) -------------------------
+            T gk[MG_N];
+            for (int e = 0; e < MG_N; ++e) gk[e] = T(0);
             if (S || (k >= 0 && k <= ni)) {
-                long f = (long)k * nj + gj;
-                txk = (T)(PIPE ? B->tx[lane] : ld(I.tnx + f));
-                tyk = (T)(PIPE ? B->ty[lane] : ld(I.tny + f));
+                if constexpr (PIPE) {
+                    for (int ch = 0; ch < MarchRow<T>::RCH; ++ch)
+                        for (int e = 0; e < MarchRow<T>::EPC; ++e) gk[ch * MarchRow<T>::EPC + e] = B->rec[ch][lane][e];
+                } else {
+                    const T* g = I.mg + MG_N * ((long)k * nj + gj);
+                    for (int e = 0; e < MG_N; ++e) gk[e] = ld(g + e);
+                }
             }
+            const T txk = gk[MG_TX], tyk = gk[MG_TY];
 
             // ---- gradients, diffusion tensor, SA source of row r = k-1 -----
             const int r = k - 1;
@@ -339,11 +365,10 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             T snew = T(0), nxr = T(0), nyr = T(0);
             if (S || (r >= i0 - 1 && r <= i1)) {
                 if (S || (r >= 0 && r < ni)) {
-                    const long id = (long)r * nj + gj;
-                    nxr = (T)(PIPE ? B->nx[lane] : ld(I.nnx + id));
-                    nyr = (T)(PIPE ? B->ny[lane] : ld(I.nny + id));
+                    nxr = gk[MG_NX];
+                    nyr = gk[MG_NY];
                     const T rtx = jst_shfl_down(nxr, 1), rty = jst_shfl_down(nyr, 1);
-                    const T iv = (T)(PIPE ? B->iv[lane] : ld(I.inv_vol + id));
+                    const T iv = gk[MG_IV];
                     T g[8];
                     for (int q = 0; q < 4; ++q) {
                         const T cq = qw[1][q];
@@ -367,9 +392,8 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     dn[6] = d.dy3;
                     dn[7] = d.dy4;
                     if (S || (r >= i0 && r < i1)) {
-                        T s5 = sa_source<T>(u[3][0], u[3][4], (T)(PIPE ? B->d2[lane] : ld(I.inv_d2 + id)), d.chi,
-                                            d.fv1, g[2], g[1], g[6], g[7], c);
-                        snew = s5 * (T)(PIPE ? B->vol[lane] : ld(I.vol + id));
+                        T s5 = sa_source<T>(u[3][0], u[3][4], gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
+                        snew = s5 * gk[MG_VOL];
                     }
                     if (!S && r == 0) {
                         // the wall ghost ring (row -1, one row up in the window) takes cell
@@ -519,7 +543,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         T bb = T(0.5) * (ty[0] + ty[1]);
                         T cc = T(0.5) * (nx2[0] + nxr3);
                         T dd = T(0.5) * (ny2[0] + nyr3);
-                        T vol = (T)(PIPE ? B->volm[lane] : ld(I.vol + id));
+                        T vol = PIPE ? B->volm[lane] : ld(I.mg + MG_N * (id + nj) + MG_VOL);
                         T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
                         T dl = local_dt<T>(qvx, qvy, sqrt((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
                         ratio_next[id] = vol / dl;
