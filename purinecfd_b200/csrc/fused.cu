@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -145,10 +146,10 @@ void launch_wall_force(const Geom& g, const UnPtrs& up, const PhysConst& c, doub
 
 // Tile configurations compiled into the library: (TI, TJ, NT).
 #define JST_FOR_TILES(X) X(4, 32, 256) X(8, 32, 256) X(16, 32, 256) X(4, 64, 256) X(8, 64, 256) X(8, 32, 192) X(8, 32, 128) X(16, 32, 384)
-// Marching-strip configurations: (rows per strip H, threads per block).  A
-// strip is fused::MARCH_W = 26 columns wide, so these are selected by
-// tile_j == 26, tile_i == H.
-#define JST_FOR_MARCH(X) X(16, 128) X(32, 128) X(64, 128) X(32, 256) X(32, 64)
+// Marching-strip configurations: threads per block.  A strip is
+// fused::MARCH_W = 26 columns wide, so these are selected by tile_j == 26;
+// tile_i is the (maximum) strip height, a run-time choice.
+#define JST_FOR_MARCH(X) X(64) X(128) X(256)
 
 template <class T> struct Kernels {
     void (*stage[3])(const TileRef*, int*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};
@@ -169,12 +170,12 @@ template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
     return k;
 }
 
-template <class T, int H, int NT> Kernels<T> march_kernels_for() {
+template <class T, int NT> Kernels<T> march_kernels_for() {
     constexpr bool PIPE = true;
     Kernels<T> k;
-    k.stage[0] = fused::k_march<T, H, NT, true, false, PIPE>;
-    k.stage[1] = fused::k_march<T, H, NT, false, false, PIPE>;
-    k.stage[2] = fused::k_march<T, H, NT, false, true, PIPE>;
+    k.stage[0] = fused::k_march<T, NT, true, false, PIPE>;
+    k.stage[1] = fused::k_march<T, NT, false, false, PIPE>;
+    k.stage[2] = fused::k_march<T, NT, false, true, PIPE>;
     k.step_dt = fused::k_step_dt<T, NT>;
     k.smem = fused::march_smem_bytes<T, NT, PIPE>();
     k.nt = NT;
@@ -190,9 +191,9 @@ template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 2
     }
     JST_FOR_TILES(JST_PICK)
 #undef JST_PICK
-#define JST_PICK_MARCH(h, n)                                        \
-    if (ti == h && tj == fused::MARCH_W && nt == n) {               \
-        *out = march_kernels_for<T, h, n>();                        \
+#define JST_PICK_MARCH(n)                                           \
+    if (ti >= 4 && ti <= 1024 && tj == fused::MARCH_W && nt == n) { \
+        *out = march_kernels_for<T, n>();                           \
         return true;                                                \
     }
     JST_FOR_MARCH(JST_PICK_MARCH)
@@ -228,10 +229,10 @@ void default_tile(int prec, int nj, int* ti, int* tj) {
 }
 
 // Tile configurations the autotuner times, in order (TI, TJ, threads).
-// Marching candidates are (H, 26, threads).
+// Marching candidates are (maximum strip height, 26, threads).
 const int kTileCands[][3] = {{8, 32, 256}, {8, 32, 192}, {16, 32, 384}, {16, 32, 256}, {4, 32, 256},
-                             {4, 64, 256},  {8, 64, 256}, {8, 32, 128}, {32, 26, 128}, {16, 26, 128},
-                             {64, 26, 128}, {32, 26, 64}};
+                             {4, 64, 256},  {8, 64, 256}, {8, 32, 128}, {16, 26, 64},  {24, 26, 64},
+                             {32, 26, 64},  {48, 26, 64}, {64, 26, 64}, {32, 26, 128}};
 
 // Stage input buffer = T copy of U_n, so a middle stage can be timed without
 // touching the solution.
@@ -252,9 +253,48 @@ std::vector<TileRef> make_tiles(int inst, int ni, int nj, int ti, int tj) {
     std::vector<TileRef> t;
     int a_n = (ni + ti - 1) / ti, b_n = (nj + tj - 1) / tj;
     t.reserve((size_t)a_n * b_n);
-    for (int a = 0; a < a_n; ++a)
-        for (int b = 0; b < b_n; ++b) t.push_back(TileRef{inst, a * ti, b * tj, a * b_n + b});
+    for (int a = 0; a < a_n; ++a) {
+        // marching strips: a_n bands of nearly equal height (at most ti rows)
+        int i0 = tj == fused::MARCH_W ? (int)((long)a * ni / a_n) : a * ti;
+        int i1 = tj == fused::MARCH_W ? (int)((long)(a + 1) * ni / a_n) : std::min(a * ti + ti, ni);
+        for (int b = 0; b < b_n; ++b) t.push_back(TileRef{inst, i0, b * tj, a * b_n + b, i1});
+    }
     return t;
+}
+
+// Most work items any configuration the autotuner may pick cuts an NI x NJ
+// mesh into (the fixed candidates, and strips of the smallest modelled height).
+int tuned_tiles_bound(int ni, int nj) {
+    int m = ((ni + 7) / 8) * ((nj + fused::MARCH_W - 1) / fused::MARCH_W);
+    for (const auto& cd : kTileCands) m = std::max(m, ((ni + cd[0] - 1) / cd[0]) * ((nj + cd[1] - 1) / cd[1]));
+    return m;
+}
+
+// Strip height for the marching kernels from a wave model: warps take strips
+// from a counter, so a launch lasts about ceil(strips / resident warps)
+// strip walks of (rows + 6) rows each.  Returns the height in [8, 128] that
+// minimises that over the given instances (nearly equal bands per instance).
+int march_height(const std::vector<std::pair<int, std::pair<int, int>>>& insts, long resident_warps) {
+    int best_h = 32;
+    double best = 1e300;
+    for (int h = 8; h <= 128; ++h) {
+        long strips = 0;
+        double rows = 0.0;
+        for (const auto& in : insts) {
+            long cols = (in.second.second + fused::MARCH_W - 1) / fused::MARCH_W;
+            long bands = (in.second.first + h - 1) / h;
+            strips += bands * cols;
+            rows += (double)in.second.first * cols;
+        }
+        if (strips == 0) return best_h;
+        long waves = (strips + resident_warps - 1) / std::max(1L, resident_warps);
+        double cost = (double)waves * (rows / (double)strips + 6.0);
+        if (cost < best) {
+            best = cost;
+            best_h = h;
+        }
+    }
+    return best_h;
 }
 
 // Times one middle-stage launch per candidate over the given instances
@@ -272,7 +312,21 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (const auto& cand : kTileCands) {
+    std::vector<std::array<int, 3>> cands;
+    for (const auto& cd : kTileCands) cands.push_back({cd[0], cd[1], cd[2]});
+    {
+        Kernels<T> K;
+        int occ = 1;
+        if (pick_kernels<T>(32, fused::MARCH_W, &K, 64) &&
+            cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K.stage[1], K.nt, K.smem) == cudaSuccess) {
+            int h = march_height(insts, (long)sms * occ * (K.nt / 32));
+            cands.push_back({h, fused::MARCH_W, 64});
+            cands.push_back({h, fused::MARCH_W, 128});
+        }
+        cudaGetLastError();
+    }
+    for (const auto& cand : cands) {
         Kernels<T> K;
         if (!pick_kernels<T>(cand[0], cand[1], &K, cand[2])) continue;
         if (cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) != cudaSuccess) {
@@ -398,9 +452,7 @@ template <class T> class FusedEngine : public Engine {
         std::vector<TileRef> tiles = make_tiles(0, ni, nj, ti, tj);
         ntiles_ = (int)tiles.size();
         int max_tiles = ntiles_;  // the autotuner may pick a smaller tile
-        if (tune_)
-            for (const auto& cd : kTileCands)
-                max_tiles = std::max(max_tiles, ((ni + cd[0] - 1) / cd[0]) * ((nj + cd[1] - 1) / cd[1]));
+        if (tune_) max_tiles = std::max(max_tiles, tuned_tiles_bound(ni, nj));
         size_t n = (size_t)ni * nj;
         size_t bytes = 0;
         auto add = [&](size_t b) {
@@ -1050,8 +1102,7 @@ template <class T> class Batch : public BatchBase {
 
     int max_tiles_for(int ni, int nj) const {
         int m = ((ni + ti_ - 1) / ti_) * ((nj + tj_ - 1) / tj_);
-        if (tune_)
-            for (const auto& cd : kTileCands) m = std::max(m, ((ni + cd[0] - 1) / cd[0]) * ((nj + cd[1] - 1) / cd[1]));
+        if (tune_) m = std::max(m, tuned_tiles_bound(ni, nj));
         return m;
     }
 
@@ -1230,8 +1281,7 @@ template <class T> class Batch : public BatchBase {
             cudaMemcpyAsync(d_states_ + slot, &h_states_[slot], sizeof(InstState), cudaMemcpyHostToDevice, st_);
             cudaMemcpyAsync(d_insts_ + slot, &h_insts_[slot], sizeof(Inst<T>), cudaMemcpyHostToDevice, st_);
             int tile_off = (int)h_tiles_.size();
-            for (int a = 0; a < tiles_i; ++a)
-                for (int b = 0; b < tiles_j; ++b) h_tiles_.push_back(TileRef{slot, a * ti_, b * tj_, a * tiles_j + b});
+            for (const TileRef& t : make_tiles(slot, ni, nj, ti_, tj_)) h_tiles_.push_back(t);
             counts_tmp_ = ntl;
             cudaMemcpyAsync(d_counts_ + slot, &counts_tmp_, sizeof(int), cudaMemcpyHostToDevice, st_);
             cudaMemcpyAsync(d_tiles_ + tile_off, h_tiles_.data() + tile_off, ntl * sizeof(TileRef),

@@ -93,6 +93,7 @@ template <class T> struct Inst {
 
 struct TileRef {
     int inst, i0, j0, tile;  // tile = index within its instance
+    int i1;                  // end row (exclusive): rows i0 .. i1-1 belong to this item
 };
 
 // Shared-memory layout of one tile.  T-typed arrays first, then the FP64
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(NT) k_step_dt(const TileRef* tiles, const int*
     double mloc = __longlong_as_double(0x7ff0000000000000LL);
     for (int w = JST_TID(); w < TI * TJ; w += NT) {
         int i = tr.i0 + w / TJ, j = tr.j0 + w % TJ;
-        if (i >= I.ni || j >= I.nj) continue;
+        if (i >= tr.i1 || j >= I.nj) continue;
         long id = (long)i * I.nj + j;
         double u, v, t;
         if (fresh) {

@@ -1,11 +1,12 @@
 // Warp-marching stage kernel: the same RK stage as k_stage (fused_kernels.cuh),
 // organised for instruction economy instead of shared-memory tiles.
 //
-// Work item = a strip of 26 output columns (j0 .. j0+25) and up to H rows
-// (i0 .. i0+H-1) of one instance.  One warp owns a strip: lane L holds column
+// Work item = a strip of 26 output columns (j0 .. j0+25) and the rows
+// i0 .. i1-1 of one instance (the host cuts each instance into bands of
+// nearly equal height, chosen so that the strips fill whole waves of warps).  One warp owns a strip: lane L holds column
 // j0-3+L (a 3-column halo on each side), so every j-neighbour the stencil
 // needs is one or two lanes away and comes from a register shuffle; the warp
-// walks down the rows i0-3 .. i0+H+2 keeping sliding windows of the rows it
+// walks down the rows i0-3 .. i1+2 keeping sliding windows of the rows it
 // still needs in registers (U: 4 rows, primitives: 2, sensors: 3, diffusion
 // tensors: 2, the previous tau-face flux).  Every value is loaded from HBM
 // once per strip and computed once per cell (plus a 6-row warm-up and the
@@ -132,7 +133,7 @@ template <class T, int NT> constexpr int march_min_blocks() {
 // PIPE: every global input of row k+1 is copied into a per-warp shared
 // buffer (cp.async) while row k is computed, so the walk never waits on HBM
 // latency; without PIPE the loads are issued in the row that uses them.
-template <class T, int H, int NT, bool FIRST, bool LAST, bool PIPE = false>
+template <class T, int NT, bool FIRST, bool LAST, bool PIPE = false>
 __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage,
                                               double alpha) {
     using TD = typename std::conditional<LAST, double, T>::type;
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             else dst[v] = reinterpret_cast<TD*>((stage % 2 == 0) ? I.ua[v] : I.ub[v]);
         }
 
-        const int i1 = i0 + H < ni ? i0 + H : ni;  // output rows i0 .. i1-1
+        const int i1 = tr.i1;                       // output rows i0 .. i1-1
         const int cu = j0 - 3 + lane;               // unwrapped column of this lane
         const int gj = wrapj(cu, nj);
         const bool seam = cu < 0 || cu >= nj;

@@ -79,7 +79,8 @@ def test_fused_tile_shape_invariance_bitwise(tile):
 
 
 @pytest.mark.parametrize("cfgt", [(4, 32, 256), (8, 32, 128), (8, 32, 192), (16, 32, 384), (8, 64, 256),
-                                  (16, 26, 128), (32, 26, 128), (64, 26, 128), (32, 26, 256), (32, 26, 64)],
+                                  (16, 26, 128), (32, 26, 128), (64, 26, 128), (32, 26, 256), (32, 26, 64),
+                                  (11, 26, 64), (48, 26, 64)],
                          ids=lambda t: "x".join(map(str, t)))
 def test_fused_every_compiled_configuration_matches_oracle(cfgt):
     """Every tile shape and block size the autotuner may pick (block sizes
