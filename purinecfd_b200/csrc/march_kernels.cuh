@@ -115,8 +115,15 @@ template <class T> struct MarchRow {
     T volm[32];                       // V of row k-3 (last stage)
 };
 
+// FP64 keeps the 4-row U window in a per-warp shared ring of 5 rows (the
+// registers it would take push the FP64 kernel past 255 registers).
+template <class T> JST_HD constexpr bool march_u_ring() { return sizeof(T) == sizeof(double); }
+template <class T> struct MarchURing {
+    T u[5][5][32];  // [row slot][variable][lane]
+};
+
 template <class T, int NT, bool PIPE> constexpr size_t march_smem_bytes() {
-    return PIPE ? (size_t)(NT / 32) * 2 * sizeof(MarchRow<T>) : 0;
+    return (size_t)(NT / 32) * ((PIPE ? 2 * sizeof(MarchRow<T>) : 0) + (march_u_ring<T>() ? sizeof(MarchURing<T>) : 0));
 }
 
 // Minimum resident blocks per SM asked of the register allocator: 12 warps
@@ -138,10 +145,15 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                                               double alpha) {
     using TD = typename std::conditional<LAST, double, T>::type;
     const int lane = JST_LANE();
+    constexpr bool UR = march_u_ring<T>();
     MarchRow<T>* rowbuf = nullptr;
-    if constexpr (PIPE) {
+    MarchURing<T>* uring = nullptr;
+    if constexpr (PIPE || UR) {
         JST_DYN_SMEM(smem_raw);
-        rowbuf = reinterpret_cast<MarchRow<T>*>(smem_raw) + 2 * JST_WARP_IN_BLOCK();
+        const int w = JST_WARP_IN_BLOCK();
+        if constexpr (PIPE) rowbuf = reinterpret_cast<MarchRow<T>*>(smem_raw) + 2 * w;
+        if constexpr (UR)
+            uring = reinterpret_cast<MarchURing<T>*>(smem_raw + (PIPE ? (size_t)(NT / 32) * 2 * sizeof(MarchRow<T>) : 0)) + w;
     }
     const int nt_all = sched[0];
     unsigned* work = reinterpret_cast<unsigned*>(sched + 1);
@@ -269,6 +281,16 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         auto row = [&](auto steady, int k) {
             constexpr bool S = decltype(steady)::value;
             const MarchRow<T>* B = nullptr;
+            // U of row k-4+a (a = 0..3): the register window, or the ring slot
+            const int s0 = UR ? ((k % 5) + 5) % 5 : 0;  // ring slot of row k
+            auto UA = [&](int a, int v) -> T {
+                if constexpr (UR) {
+                    int sl = s0 + 1 + a;
+                    return uring->u[sl >= 5 ? sl - 5 : sl][v][lane];
+                } else {
+                    return u[a][v];
+                }
+            };
             if constexpr (PIPE) {
                 if (S) issue(steady, k + 1);
                 else if (k + 1 <= i1 + 2) issue(std::false_type{}, k + 1);
@@ -335,7 +357,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 qk[2] = q.t;
                 qk[3] = q.nut;
             } else {  // rows ni+1, ni+2 repeat row ni
-                for (int v = 0; v < 5; ++v) uk[v] = u[3][v];
+                for (int v = 0; v < 5; ++v) uk[v] = UA(3, v);
                 pk = pw[1];
                 for (int v = 0; v < 4; ++v) qk[v] = qw[1][v];
             }
@@ -381,7 +403,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                             green_gauss_delta<T>(cq, qk[q], qw[0][q], lf, rg, txk, tyk, tx[2], ty[2], nxr, nyr, rtx,
                                                  rty, iv, &g[2 * q], &g[2 * q + 1]);
                     }
-                    Diff<T> d = diffusion_tensor<T>(qw[1][2], u[3][4], qw[1][0], qw[1][1], g[0], g[1], g[2], g[3], g[4],
+                    Diff<T> d = diffusion_tensor<T>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], g[0], g[1], g[2], g[3], g[4],
                                                     g[5], g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num, (T)c.t_suth,
                                                     (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp, (T)c.sigma);
                     dn[0] = d.dx1;
@@ -393,13 +415,13 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     dn[6] = d.dy3;
                     dn[7] = d.dy4;
                     if (S || (r >= i0 && r < i1)) {
-                        T s5 = sa_source<T>(u[3][0], u[3][4], gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
+                        T s5 = sa_source<T>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
                         snew = s5 * gk[MG_VOL];
                     }
                     if (!S && r == 0) {
                         // the wall ghost ring (row -1, one row up in the window) takes cell
                         // 0's gradient with grad T = 0 (gradient.rs:93-95)
-                        Diff<T> w = diffusion_tensor<T>(qw[0][2], u[2][4], qw[0][0], qw[0][1], g[0], g[1], g[2], g[3],
+                        Diff<T> w = diffusion_tensor<T>(qw[0][2], UA(2, 4), qw[0][0], qw[0][1], g[0], g[1], g[2], g[3],
                                                         T(0), T(0), g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num,
                                                         (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt,
                                                         (T)c.cp, (T)c.sigma);
@@ -413,7 +435,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         dw[1][7] = w.dy4;
                     }
                 } else if (r >= ni) {  // far ghost ring: zero gradient (gradient.rs:96)
-                    Diff<T> d = diffusion_tensor<T>(qw[1][2], u[3][4], qw[1][0], qw[1][1], T(0), T(0), T(0), T(0),
+                    Diff<T> d = diffusion_tensor<T>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], T(0), T(0), T(0), T(0),
                                                     T(0), T(0), T(0), T(0), (T)c.inv_t_ref, (T)c.suth_num,
                                                     (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp,
                                                     (T)c.sigma);
@@ -447,13 +469,20 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 T e4 = tmax<T>(k4 - e2, T(0));
                 T lam = half_cfl * (rtn + rt0);
                 T fu[5], cv[5];
-                for (int v = 0; v < 5; ++v) fu[v] = T(0.5) * (u[1][v] + u[2][v]);
+                T w0[5], w1[5], w2[5], w3[5];
+                for (int v = 0; v < 5; ++v) {
+                    w0[v] = UA(0, v);
+                    w1[v] = UA(1, v);
+                    w2[v] = UA(2, v);
+                    w3[v] = UA(3, v);
+                    fu[v] = T(0.5) * (w1[v] + w2[v]);
+                }
                 const T fnx = tx[1], fny = ty[1];
                 euler_flux<T>(fu, fnx, fny, gm1, cv, p_ref);
                 T hx = T(0.5) * fnx, hy = T(0.5) * fny;
                 for (int v = 0; v < 5; ++v) {
-                    T d1 = u[2][v] - u[1][v];
-                    T d3 = u[3][v] - T(3) * u[2][v] + T(3) * u[1][v] - u[0][v];
+                    T d1 = w2[v] - w1[v];
+                    T d3 = w3[v] - T(3) * w2[v] + T(3) * w1[v] - w0[v];
                     T vis = T(0);
                     if (v > 0) vis = (dw[0][v - 1] + dw[1][v - 1]) * hx + (dw[0][v + 3] + dw[1][v + 3]) * hy;
                     ftn[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
@@ -471,20 +500,21 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     T e2 = k2 * m4;
                     T e4 = tmax<T>(k4 - e2, T(0));
                     T lam = half_cfl * (rt0 + jst_shfl_up(rt0, 1));
-                    T ul1[5], ul2[5], ur1[5], fu[5], cv[5];
+                    T ul1[5], ul2[5], ur1[5], fu[5], cv[5], um[5];
                     for (int v = 0; v < 5; ++v) {
-                        ul1[v] = jst_shfl_up(u[1][v], 1);
-                        ul2[v] = jst_shfl_up(u[1][v], 2);
-                        ur1[v] = jst_shfl_down(u[1][v], 1);
-                        fu[v] = T(0.5) * (ul1[v] + u[1][v]);
+                        um[v] = UA(1, v);
+                        ul1[v] = jst_shfl_up(um[v], 1);
+                        ul2[v] = jst_shfl_up(um[v], 2);
+                        ur1[v] = jst_shfl_down(um[v], 1);
+                        fu[v] = T(0.5) * (ul1[v] + um[v]);
                     }
                     euler_flux<T>(fu, nx2[0], ny2[0], gm1, cv, p_ref);
                     T hx = T(0.5) * nx2[0], hy = T(0.5) * ny2[0];
                     T dl[8];
                     for (int v = 0; v < 8; ++v) dl[v] = jst_shfl_up(dw[0][v], 1);
                     for (int v = 0; v < 5; ++v) {
-                        T d1 = u[1][v] - ul1[v];
-                        T d3 = ur1[v] - T(3) * u[1][v] + T(3) * ul1[v] - ul2[v];
+                        T d1 = um[v] - ul1[v];
+                        T d3 = ur1[v] - T(3) * um[v] + T(3) * ul1[v] - ul2[v];
                         T vis = T(0);
                         if (v > 0) vis = (dl[v - 1] + dw[0][v - 1]) * hx + (dl[v + 3] + dw[0][v + 3]) * hy;
                         fn[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
@@ -556,10 +586,14 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
 
             // ---- slide the windows ------------------------------------------
             for (int v = 0; v < 5; ++v) {
-                u[0][v] = u[1][v];
-                u[1][v] = u[2][v];
-                u[2][v] = u[3][v];
-                u[3][v] = uk[v];
+                if constexpr (UR) {
+                    uring->u[s0][v][lane] = uk[v];
+                } else {
+                    u[0][v] = u[1][v];
+                    u[1][v] = u[2][v];
+                    u[2][v] = u[3][v];
+                    u[3][v] = uk[v];
+                }
                 ft[v] = ftn[v];
             }
             nu3 = qw[0][3];
