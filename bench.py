@@ -325,8 +325,12 @@ def run_ours(args, world, rank, local):
                            "seconds": round(t_e2e, 4),
                            "what": "jst_create from host nodes + jst_run with per-step residual callback + "
                                    "6 fields read back"}
-        if world == 1 and args.batch_instances > 0:
-            line["batch"] = batched_leg(args)
+    # every rank takes part in the batch leg (its instances are dealt over the ranks)
+    if args.batch_instances > 0:
+        batch = batched_leg(args, world, rank)
+        if rank == 0:
+            line["batch"] = batch
+    if rank == 0:
         if world == 1 and not args.no_cpu:
             r = cpu_reference(args.workload, 2, 1)
             line["cpu_baseline"] = {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
@@ -335,46 +339,85 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def batched_leg(args):
+def batched_leg(args, world: int = 1, rank: int = 0):
     """Config-4 distribution: NACA 4-digit instances on three mesh classes with
     seeded M, alpha, Re (local time stepping, CFL 1.0), solved (a) all at once
     in one FP32-split batch, (b) all at once in FP64 as the CL/CD reference and
     (c) a subsample one at a time in FP64 (batch of one).  Each instance
-    retires on a 1e-6 residual drop or at the step cap."""
+    retires on a 1e-6 residual drop or at the step cap.  With several ranks the
+    instances are dealt round-robin (instance k on rank k mod N): they are
+    independent, so no data moves between GPUs; the job time is the slowest
+    rank's."""
     from purinecfd_b200 import PREC_FP32_SPLIT, PREC_FP64, workloads
-    from purinecfd_b200.serve import batch_solve, percentile
+    from purinecfd_b200.serve import batch_solve
     cases = []
-    for k in range(args.batch_instances):
+    for k in range(rank, args.batch_instances, world):
         cfg, xy, nr, nt, _ = workloads.batch_instance(20261203, k)
         cfg["simulation"]["CFL"] = 1.0
         cases.append((cfg, xy, nr, nt))
-    cells = sum((c[2] - 1) * c[3] for c in cases)
-    split, t_split = batch_solve(cases, PREC_FP32_SPLIT, max_steps=args.batch_steps)
-    ref, t_ref = batch_solve(cases, PREC_FP64, max_steps=args.batch_steps)
-    m = max(1, min(args.plain_instances, len(cases)))
-    plain, t_plain = batch_solve(cases[:m], PREC_FP64, max_instances=1, max_steps=args.batch_steps)
+    part = {"instances": len(cases), "cells": sum((c[2] - 1) * c[3] for c in cases)}
+    barrier(world)
+    split, part["wall_split"] = batch_solve(cases, PREC_FP32_SPLIT, max_steps=args.batch_steps) if cases else ([], 0.0)
+    barrier(world)
+    ref, part["wall_ref"] = batch_solve(cases, PREC_FP64, max_steps=args.batch_steps) if cases else ([], 0.0)
+    part["plain_m"], part["plain_wall"] = 0, 0.0
+    if rank == 0 and cases:
+        m = max(1, min(args.plain_instances, len(cases)))
+        _, part["plain_wall"] = batch_solve(cases[:m], PREC_FP64, max_instances=1, max_steps=args.batch_steps)
+        part["plain_m"] = m
     dcl, dcd = [], []
     for a, r in zip(split, ref):
         if a.status != 8 and r.status != 8:
             dcl.append(abs(a.cl - r.cl))
             dcd.append(abs(a.cd - r.cd))
-    within = sum(1 for x, y in zip(dcl, dcd) if x <= 1e-4 and y <= 1e-4)
-    lat = [r.t_done - r.t_submit for r in split]
-    steps_split = sum(r.steps for r in split)
-    return {"instances": len(cases), "cells": cells, "step_cap": args.batch_steps,
-            "solves_per_s": round(len(cases) / t_split, 3), "wall_s": round(t_split, 3),
-            "mcell_stage_per_s": round(sum((r.ni * r.nj) * r.steps for r in split) * 5 / t_split / 1e6, 1),
-            "p50_s": round(percentile(lat, 50), 3), "p99_s": round(percentile(lat, 99), 3),
-            "converged": sum(1 for r in split if r.status == 0), "nonphysical": sum(1 for r in split if r.status == 8),
-            "mean_steps": round(steps_split / len(split), 1),
-            "fp64_batch_solves_per_s": round(len(cases) / t_ref, 3),
-            "plain_fp64_one_at_a_time": {"instances": m, "solves_per_s": round(m / t_plain, 3),
-                                         "wall_s": round(t_plain, 3)},
-            "speedup_vs_plain": round((len(cases) / t_split) / (m / t_plain), 2),
-            "cl_err_max": max(dcl) if dcl else None, "cd_err_max": max(dcd) if dcd else None,
-            "within_1e-4": f"{within}/{len(cases)}",
-            "what": "seed 20261203, PCG64 stream per instance; local time step; retire at residual drop 1e-6 "
-                    "or step cap; CL/CD error vs the FP64 batch on the same instances"}
+    part.update(cell_steps=sum((r.ni * r.nj) * r.steps for r in split), steps=sum(r.steps for r in split),
+                converged=sum(1 for r in split if r.status == 0), nonphysical=sum(1 for r in split if r.status == 8),
+                within=sum(1 for x, y in zip(dcl, dcd) if x <= 1e-4 and y <= 1e-4),
+                dcl_max=max(dcl) if dcl else None, dcd_max=max(dcd) if dcd else None,
+                latencies=[r.t_done - r.t_submit for r in split])
+    parts = gather_objects(part, world)
+    return combine_batch_parts(parts, args.batch_steps) if rank == 0 else None
+
+
+def gather_objects(obj, world: int) -> list:
+    if world == 1:
+        return [obj]
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, obj)
+    return out
+
+
+def combine_batch_parts(parts: list, step_cap: int) -> dict:
+    """Job-level batch figures from the per-rank parts."""
+    from purinecfd_b200.serve import percentile
+    world = len(parts)
+    n = sum(p["instances"] for p in parts)
+    wall = max(p["wall_split"] for p in parts)
+    wall_ref = max(p["wall_ref"] for p in parts)
+    lat = [x for p in parts for x in p["latencies"]]
+    p0 = parts[0]
+    plain_sps = p0["plain_m"] / p0["plain_wall"] if p0["plain_wall"] > 0 else None
+    errs = [p["dcl_max"] for p in parts if p["dcl_max"] is not None]
+    errd = [p["dcd_max"] for p in parts if p["dcd_max"] is not None]
+    out = {"instances": n, "ranks": world, "cells": sum(p["cells"] for p in parts), "step_cap": step_cap,
+           "solves_per_s": round(n / wall, 3) if wall > 0 else None, "wall_s": round(wall, 3),
+           "mcell_stage_per_s": round(sum(p["cell_steps"] for p in parts) * 5 / wall / 1e6, 1) if wall > 0 else None,
+           "p50_s": round(percentile(lat, 50), 3), "p99_s": round(percentile(lat, 99), 3),
+           "converged": sum(p["converged"] for p in parts), "nonphysical": sum(p["nonphysical"] for p in parts),
+           "mean_steps": round(sum(p["steps"] for p in parts) / max(1, n), 1),
+           "fp64_batch_solves_per_s": round(n / wall_ref, 3) if wall_ref > 0 else None,
+           "plain_fp64_one_at_a_time": {"instances": p0["plain_m"],
+                                        "solves_per_s_per_gpu": None if plain_sps is None else round(plain_sps, 3),
+                                        "solves_per_s_job": None if plain_sps is None else round(plain_sps * world, 3),
+                                        "wall_s": round(p0["plain_wall"], 3)},
+           "speedup_vs_plain": round((n / wall) / (plain_sps * world), 2) if plain_sps and wall > 0 else None,
+           "cl_err_max": max(errs) if errs else None, "cd_err_max": max(errd) if errd else None,
+           "within_1e-4": f"{sum(p['within'] for p in parts)}/{n}",
+           "what": "seed 20261203, PCG64 stream per instance; local time step; retire at residual drop 1e-6 "
+                   "or step cap; CL/CD error vs the FP64 batch on the same instances; instances dealt "
+                   "round-robin over the ranks, plain one-at-a-time measured on rank 0 and counted once per GPU"}
+    return out
 
 
 def serve_sweep(args):

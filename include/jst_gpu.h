@@ -176,6 +176,18 @@ jst_status jst_get_faces(jst_solver* s, int which, double* out, size_t n);
  * JST_ERR_NONPHYSICAL exactly where unpack would. */
 jst_status jst_set_conserved(jst_solver* s, const double* u5, size_t n, jst_nonphysical* bad);
 
+/* Checkpoint dump (no counterpart in the reference, whose Solver keeps no
+ * dump): writes U (5 planes, FP64), the completed step count, the physical
+ * time and the last residual to a binary file; loading it into a solver
+ * built from the same mesh continues the run where it stopped (the next
+ * step's time step is re-derived from U, as every step of the reference
+ * derives it).  File: "JSTCKPT1", int32 NI, int32 NJ, int64 step, double
+ * totaltime, double residual, 5*NI*NJ doubles, native byte order.
+ * Load fails with JST_ERR_ARG on a size mismatch or a damaged file and with
+ * JST_ERR_NONPHYSICAL like jst_set_conserved. */
+jst_status jst_checkpoint_save(jst_solver* s, const char* path);
+jst_status jst_checkpoint_load(jst_solver* s, const char* path, jst_nonphysical* bad);
+
 /* Lift and drag coefficients of the current state (no counterpart in the
  * reference): wall pressure and viscous face fluxes integrated over ring 0,
  * rotated by the angle of attack and divided by 0.5*rho_inf*V_inf^2*chord,

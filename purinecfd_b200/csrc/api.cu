@@ -236,6 +236,11 @@ class PassesEngine : public Engine {
         return cudaStreamSynchronize(core_->st) == cudaSuccess ? JST_OK : JST_ERR_CUDA;
     }
 
+    jst_status set_totaltime(double t) override {
+        cudaMemcpyAsync(passes_totaltime_ptr(P_), &t, sizeof t, cudaMemcpyHostToDevice, core_->st);
+        return cudaStreamSynchronize(core_->st) == cudaSuccess ? JST_OK : JST_ERR_CUDA;
+    }
+
     void set_uniform(double rho, double vx, double vy, double p, double nut) override {
         passes_set_uniform(P_, core_->c, rho, vx, vy, p, nut, core_->st);
     }
@@ -564,6 +569,76 @@ jst_status jst_get_faces(jst_solver* s, int which, double* out, size_t n) {
 jst_status jst_set_conserved(jst_solver* s, const double* u5, size_t n, jst_nonphysical* bad) {
     if (!s || !u5 || n < 5 * (size_t)s->core.ni * s->core.nj) return JST_ERR_ARG;
     return s->eng->set_conserved(u5, bad);
+}
+
+namespace {
+const char kCkptMagic[8] = {'J', 'S', 'T', 'C', 'K', 'P', 'T', '1'};
+void ckpt_error(jst_solver* s, const std::string& msg) {
+    s->err = msg;
+    set_call_error(msg);
+}
+}
+
+jst_status jst_checkpoint_save(jst_solver* s, const char* path) {
+    if (!s || !path) return JST_ERR_ARG;
+    const size_t n = (size_t)s->core.ni * s->core.nj;
+    std::vector<double> u(5 * n);
+    for (int k = 0; k < 5; ++k)
+        if (!s->eng->get_field(JST_F_U0 + k, u.data() + k * n)) {
+            ckpt_error(s, "cannot read the conserved state");
+            return JST_ERR_CUDA;
+        }
+    double tt = 0.0, res = std::numeric_limits<double>::quiet_NaN();
+    if (s->eng->totaltime(&tt) != JST_OK) return JST_ERR_CUDA;
+    if (s->step > 0) s->eng->residual(&res);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        ckpt_error(s, std::string("cannot create ") + path);
+        return JST_ERR_ARG;
+    }
+    int32_t dims[2] = {s->core.ni, s->core.nj};
+    int64_t step = s->step;
+    bool ok = std::fwrite(kCkptMagic, 1, 8, f) == 8 && std::fwrite(dims, sizeof dims, 1, f) == 1 &&
+              std::fwrite(&step, sizeof step, 1, f) == 1 && std::fwrite(&tt, sizeof tt, 1, f) == 1 &&
+              std::fwrite(&res, sizeof res, 1, f) == 1 && std::fwrite(u.data(), sizeof(double), u.size(), f) == u.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) {
+        ckpt_error(s, std::string("cannot write ") + path);
+        return JST_ERR_ARG;
+    }
+    return JST_OK;
+}
+
+jst_status jst_checkpoint_load(jst_solver* s, const char* path, jst_nonphysical* bad) {
+    if (!s || !path) return JST_ERR_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) {
+        ckpt_error(s, std::string("cannot open ") + path);
+        return JST_ERR_ARG;
+    }
+    char magic[8];
+    int32_t dims[2];
+    int64_t step = 0;
+    double tt = 0.0, res = 0.0;
+    const size_t n = (size_t)s->core.ni * s->core.nj;
+    std::vector<double> u(5 * n);
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCkptMagic, 8) == 0 &&
+              std::fread(dims, sizeof dims, 1, f) == 1 && dims[0] == s->core.ni && dims[1] == s->core.nj &&
+              std::fread(&step, sizeof step, 1, f) == 1 && step >= 0 && std::fread(&tt, sizeof tt, 1, f) == 1 &&
+              std::fread(&res, sizeof res, 1, f) == 1 && std::fread(u.data(), sizeof(double), u.size(), f) == u.size();
+    std::fclose(f);
+    if (!ok) {
+        ckpt_error(s, std::string(path) + ": not a checkpoint of a " + std::to_string(s->core.ni) + " x " +
+                       std::to_string(s->core.nj) + " mesh, or truncated");
+        return JST_ERR_ARG;
+    }
+    jst_nonphysical tmp{};
+    jst_status rc = s->eng->set_conserved(u.data(), bad ? bad : &tmp);
+    if (rc != JST_OK) return rc;
+    rc = s->eng->set_totaltime(tt);
+    if (rc != JST_OK) return rc;
+    s->step = step;
+    return JST_OK;
 }
 
 jst_status jst_forces(jst_solver* s, double* cl, double* cd) {

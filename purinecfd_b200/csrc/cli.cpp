@@ -27,6 +27,7 @@ std::string rexp(double v, int prec) {
 
 struct Cli {
     std::string mesh = "fangdata.txt", config = "config.json", out = "result.csv", reslog = "res.log";
+    std::string checkpoint, restart;
     long steps = -1;
     bool quiet = false, no_output = false;
     long threads = 0;
@@ -50,6 +51,8 @@ void usage() {
         "      --dt <global|local>      time step mode [default: global]\n"
         "      --path <fused|passes>    kernels [default: fused]\n"
         "      --device <N>             CUDA device [default: 0]\n"
+        "      --restart <FILE>         continue from a checkpoint written by --checkpoint\n"
+        "      --checkpoint <FILE>      write a checkpoint after the run\n"
         "  -h, --help                   Print help");
 }
 
@@ -85,6 +88,8 @@ bool parse(int argc, char** argv, Cli& c) {
         else if (a == "--dt") c.dt_mode = val() == "local" ? JST_DT_LOCAL : JST_DT_GLOBAL;
         else if (a == "--path") c.path = val() == "passes" ? JST_PATH_PASSES : JST_PATH_FUSED;
         else if (a == "--device") c.device = (int)std::strtol(val().c_str(), nullptr, 10);
+        else if (a == "--restart") c.restart = val();
+        else if (a == "--checkpoint") c.checkpoint = val();
         else {
             std::fprintf(stderr, "error: unexpected argument '%s' found\n", a.c_str());
             return false;
@@ -96,10 +101,12 @@ bool parse(int argc, char** argv, Cli& c) {
 struct LogCtx {
     FILE* log;
     bool quiet;
+    uint64_t offset;  // steps completed before this run (restart)
 };
 
 void on_step(void* user, uint64_t step, double res) {
     LogCtx* c = static_cast<LogCtx*>(user);
+    step += c->offset;
     if (!c->quiet) std::printf("step:%6llu | residual:%s\n", (unsigned long long)step, rexp(res, 6).c_str());
     if (c->log) std::fprintf(c->log, "%llu,%s\n", (unsigned long long)step, rexp(res, 6).c_str());
 }
@@ -124,7 +131,19 @@ int main(int argc, char** argv) {
     int ni = jst_ni(s), nj = jst_nj(s);
     std::printf("mesh %s: %d rings x %d points -> %lld cells\n", cli.mesh.c_str(), ni + 1, nj, (long long)ni * nj);
     std::printf("threads: %ld\n", cli.threads > 0 ? cli.threads : 1L);
-    LogCtx ctx{nullptr, cli.quiet};
+    LogCtx ctx{nullptr, cli.quiet, 0};
+    if (!cli.restart.empty()) {
+        jst_nonphysical bad0{};
+        if (jst_checkpoint_load(s, cli.restart.c_str(), &bad0) != JST_OK) {
+            std::fprintf(stderr, "Error: %s\n", jst_last_error(nullptr));
+            jst_destroy(s);
+            return 1;
+        }
+        int64_t done0 = 0;
+        jst_step_count(s, &done0);
+        ctx.offset = (uint64_t)done0;
+        std::printf("restarted from %s at step %lld\n", cli.restart.c_str(), (long long)done0);
+    }
     if (!cli.no_output) {
         ctx.log = std::fopen(cli.reslog.c_str(), "w");
         if (!ctx.log) {
@@ -150,6 +169,14 @@ int main(int argc, char** argv) {
     double per = rep.steps > 0 ? wall / (double)rep.steps : 0.0;
     std::printf("wall clock: %.6f s  (%.4f ms/step, %.1f ns/cell/step)\n", wall, per * 1e3,
                 per / ((double)ni * nj) * 1e9);
+    if (!cli.checkpoint.empty()) {
+        if (jst_checkpoint_save(s, cli.checkpoint.c_str()) != JST_OK) {
+            std::fprintf(stderr, "Error: %s\n", jst_last_error(nullptr));
+            jst_destroy(s);
+            return 1;
+        }
+        std::printf("checkpoint written to %s\n", cli.checkpoint.c_str());
+    }
     if (!cli.no_output) {
         rc = jst_write_csv(s, cli.out.c_str());
         if (rc != JST_OK) {

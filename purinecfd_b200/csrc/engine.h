@@ -49,6 +49,7 @@ class Engine {
     virtual jst_status wall_force(double* fx, double* fy) = 0;
     virtual jst_status residual(double* out) = 0;
     virtual jst_status totaltime(double* out) = 0;
+    virtual jst_status set_totaltime(double t) = 0;
     virtual jst_status time_steps(int nsteps, double* ms, double* stage_ms) {
         cudaEvent_t a, b;
         cudaEventCreate(&a);

@@ -825,6 +825,11 @@ template <class T> class FusedEngine : public Engine {
         return JST_OK;
     }
 
+    jst_status set_totaltime(double t) override {
+        cudaMemcpyAsync(&inst_.st->totaltime, &t, sizeof t, cudaMemcpyHostToDevice, core_->st);
+        return cudaStreamSynchronize(core_->st) == cudaSuccess ? JST_OK : JST_ERR_CUDA;
+    }
+
     cudaStream_t stream() const override { return core_->st; }
 
     // nsteps graph-replayed steps with the target disabled, timed with CUDA

@@ -42,7 +42,8 @@ FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
 EXPORTS = ["jst_default_opts", "jst_create_from_paths", "jst_create", "jst_destroy", "jst_last_error", "jst_ni",
            "jst_nj", "jst_advance", "jst_run", "jst_residual_terms", "jst_timestep", "jst_residual",
            "jst_totaltime", "jst_step_count", "jst_get_field", "jst_get_faces", "jst_set_conserved",
-           "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps", "jst_residual_noalloc", "jst_kernel_config"]
+           "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps", "jst_residual_noalloc", "jst_kernel_config",
+           "jst_checkpoint_save", "jst_checkpoint_load"]
 
 
 class Opts(C.Structure):
@@ -117,6 +118,8 @@ def lib() -> C.CDLL:
         L.jst_set_conserved.argtypes = [vp, pd, sz, C.POINTER(NonPhysicalC)]
         L.jst_forces.argtypes = [vp, pd, pd]
         L.jst_write_csv.argtypes = [vp, C.c_char_p]
+        L.jst_checkpoint_save.argtypes = [vp, C.c_char_p]
+        L.jst_checkpoint_load.argtypes = [vp, C.c_char_p, C.POINTER(NonPhysicalC)]
         L.jst_version.restype = C.c_char_p
         L.jst_time_steps.argtypes = [vp, i, pd, pd]
         L.jst_residual_noalloc.argtypes = [vp, vp, i, i, vp, vp]
@@ -272,6 +275,15 @@ class Solver:
     def write_csv(self, path):
         """Solver::write_csv (solver.rs:229-255)."""
         self._check(lib().jst_write_csv(self._h, str(path).encode()))
+
+    def save_checkpoint(self, path):
+        """Writes U, the step count and the physical time (no counterpart in the reference)."""
+        self._check(lib().jst_checkpoint_save(self._h, str(path).encode()))
+
+    def load_checkpoint(self, path):
+        """Continues from a checkpoint of a solver on the same mesh."""
+        bad = NonPhysicalC()
+        self._check(lib().jst_checkpoint_load(self._h, str(path).encode(), C.byref(bad)), bad)
 
     def time_steps(self, nsteps: int, stages: bool = False):
         """Device time (ms) of `nsteps` RK steps with the convergence test off,

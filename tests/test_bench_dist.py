@@ -32,8 +32,18 @@ def _rank(rank: int, world: int, port: int, q):
     ms = 100.0 + 25.0 * r  # rank 1 is the slow one
     m = bench.max_over_ranks(ms, w)
     bench.barrier(w)
-    q.put((r, w, m, bench.replica_value(1000, 10, m, w)))
+    parts = bench.gather_objects(_part(r), w)
+    q.put((r, w, m, bench.replica_value(1000, 10, m, w), parts))
     dist.destroy_process_group()
+
+
+def _part(rank: int) -> dict:
+    """A batch-leg part as one rank reports it (instances k = rank, rank + 2, ...)."""
+    return {"instances": 3 - rank, "cells": 1000 * (3 - rank), "wall_split": 2.0 + rank, "wall_ref": 5.0 - rank,
+            "plain_m": 2 if rank == 0 else 0, "plain_wall": 4.0 if rank == 0 else 0.0,
+            "cell_steps": 10_000 * (3 - rank), "steps": 30 - 10 * rank, "converged": 1, "nonphysical": rank,
+            "within": 3 - 2 * rank, "dcl_max": 1e-6 * (rank + 1), "dcd_max": None if rank else 2e-7,
+            "latencies": [1.0 + rank, 2.0 + rank]}
 
 
 def test_two_rank_barrier_and_max_over_ranks():
@@ -48,9 +58,30 @@ def test_two_rank_barrier_and_max_over_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert [o[0] for o in out] == [0, 1]
-    for r, w, m, v in out:
+    for r, w, m, v, parts in out:
         assert w == 2 and m == 125.0
         assert v == pytest.approx(2 * 1000 * 5 * 10 / 0.125 / 1e6)
+        assert parts == [_part(0), _part(1)]  # every rank sees every part, in rank order
+
+
+def test_batch_parts_combine_to_job_figures():
+    """5 instances dealt over 2 ranks: the job takes the slowest rank's wall
+    time, counts add, errors take the maximum, and the plain one-at-a-time
+    rate measured on rank 0 counts once per GPU."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    b = bench.combine_batch_parts([_part(0), _part(1)], 1000)
+    assert b["instances"] == 5 and b["ranks"] == 2 and b["cells"] == 5000
+    assert b["wall_s"] == 3.0 and b["solves_per_s"] == pytest.approx(5 / 3.0, abs=1e-3)
+    assert b["fp64_batch_solves_per_s"] == pytest.approx(1.0)
+    assert b["mcell_stage_per_s"] == pytest.approx(50_000 * 5 / 3.0 / 1e6, abs=0.1)
+    assert b["converged"] == 2 and b["nonphysical"] == 1 and b["mean_steps"] == pytest.approx(10.0)
+    assert b["cl_err_max"] == pytest.approx(2e-6) and b["cd_err_max"] == pytest.approx(2e-7)
+    assert b["within_1e-4"] == "4/5"
+    plain = b["plain_fp64_one_at_a_time"]
+    assert plain["solves_per_s_per_gpu"] == pytest.approx(0.5) and plain["solves_per_s_job"] == pytest.approx(1.0)
+    assert b["speedup_vs_plain"] == pytest.approx((5 / 3.0) / 1.0, abs=0.01)
+    assert b["p50_s"] == pytest.approx(2.0) and b["p99_s"] <= 3.0
 
 
 def test_single_rank_needs_no_process_group():
