@@ -59,7 +59,8 @@ typedef enum {
 
 /* Which kernels run a stage. */
 typedef enum {
-    JST_PATH_FUSED = 0, /* one tiled kernel per RK stage (production) */
+    JST_PATH_FUSED = 0, /* one stage kernel per RK stage (production): warp-marching
+                           strips or shared-memory tiles, chosen by the autotuner */
     JST_PATH_PASSES = 1 /* one kernel per reference pass, strict FP64 (parity mode) */
 } jst_kernel_path;
 
@@ -68,8 +69,8 @@ typedef struct {
     int dt_mode;     /* jst_dt_mode */
     int kernel_path; /* jst_kernel_path */
     int device;      /* CUDA device ordinal */
-    int tile_i;      /* fused path tile rows (0 = autotuned) */
-    int tile_j;      /* fused path tile columns (0 = autotuned) */
+    int tile_i;      /* fused path: tile rows, or maximum strip height when tile_j == 26 */
+    int tile_j;      /* fused path: tile columns; 26 selects the marching strips (0, 0 = autotuned) */
     int use_graph;   /* capture each RK step as a CUDA graph (fused path) */
     double nut_inf_ratio; /* free-stream nu-tilde / nu; <= 0 uses the config value or 0.1 */
     int block_threads;    /* fused path threads per block (0 = default for the tile) */
