@@ -42,11 +42,14 @@ UNIT = "Mcell-stage/s"
 # (U_n FP64 40 B; stage state and V/dt in the stage type T).
 # Marching kernel (the autotuner's choice on large meshes): geometry is one
 # record of 8 T per cell (tau and n normals, 1/V, 1/d^2, V, pad) plus the
-# FP64 1/V of the updated cell (8 B):
-#   split: stages 1-4: U 20 + U_n 40 + write 20 + record 32 + 1/V 8 + ratio 4       = 124
+# FP64 1/V of the updated cell (8 B).  In split precision stages 1-4 take
+# their accumulator from the FP32 copy of U_n (stage 1 already reads it as
+# its input); stage 5 adds to U_n in FP64:
+#   split: stage 1: U_n copy 20 + write 20 + record 32 + 1/V 8 + ratio 4           = 84
+#          stages 2-4: U 20 + U_n copy 20 + write 20 + record 32 + 1/V 8 + ratio 4 = 104
 #          stage 5: U 20 + U_n 40 + write U_n 40 + FP32 copy 20 + record 32 + 1/V 8
 #                   + V 4 + ratio 4+4                                               = 172
-#          average 133.6 B
+#          average 113.6 B
 #   FP64:  stage 1: U_n 40 + write 40 + record 64 + 1/V 8 + ratio 8                 = 160
 #          stages 2-4: U 40 + U_n 40 + write 40 + record 64 + 1/V 8 + ratio 8       = 200
 #          stage 5: U 40 + U_n 40 + write U_n 40 + record 64 + 1/V 8 + V 8
@@ -55,7 +58,7 @@ UNIT = "Mcell-stage/s"
 # Tile kernel: geometry = tau and n normals 32 B, V 8, 1/V 8, 1/d^2 8 = 56 B (FP64):
 #   split: stages 1-4: U 20 + U_n 40 + write 20 + geom 56 + ratio 4  = 140;  stage 5: 184;  average 148.8 B
 #   FP64:  stage 1: 144;  stages 2-4: 184;  stage 5: 192;  average 177.6 B
-BYTES_PER_STAGE = {("march", "split"): [124, 124, 124, 124, 172], ("march", "fp64"): [160, 200, 200, 200, 216],
+BYTES_PER_STAGE = {("march", "split"): [84, 104, 104, 104, 172], ("march", "fp64"): [160, 200, 200, 200, 216],
                    ("tile", "split"): [140, 140, 140, 140, 184], ("tile", "fp64"): [144, 184, 184, 184, 192]}
 
 

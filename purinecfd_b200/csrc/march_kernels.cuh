@@ -110,6 +110,7 @@ template <class T> struct MarchRow {
     static constexpr int RCH = MG_N * (int)sizeof(T) / 16, EPC = 16 / (int)sizeof(T);
     alignas(16) T rec[RCH][32][EPC];  // Inst::mg record of row k
     double un[5][32], ldt[32], ivm[32];  // U_n, dt_local, 1/V of row k-3
+    T uacc[5][32];                    // FP32 copy of U_n of row k-3 (split, stages 1-3)
     T u[5][32];                       // stage input of row k
     T rat[32];                        // V/dt of row k-2 (clamped)
     T volm[32];                       // V of row k-3 (last stage)
@@ -146,6 +147,11 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
     using TD = typename std::conditional<LAST, double, T>::type;
     const int lane = JST_LANE();
     constexpr bool UR = march_u_ring<T>();
+    // Split precision, stages 0-3: their output is stored in FP32, so the RK
+    // accumulator starts from the FP32 copy of U_n (what they store differs
+    // from rounding U_n - increment once by at most one FP32 rounding); the
+    // last stage adds its increment to U_n in FP64.
+    constexpr bool ACC32 = sizeof(T) == sizeof(float) && !LAST;
     MarchRow<T>* rowbuf = nullptr;
     MarchURing<T>* uring = nullptr;
     if constexpr (PIPE || UR) {
@@ -234,7 +240,12 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             const int m = kk - 3;
             if (S || (m >= i0 && m < i1)) {
                 const long id = (long)m * nj + gj;
-                for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[v] + id);
+                if constexpr (ACC32) {
+                    if constexpr (!FIRST)  // stage 0 reads the same values as its stage input
+                        for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.uacc[v][lane], I.uc[v] + id);
+                } else {
+                    for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[v] + id);
+                }
                 if (I.local_dt) async_copy<8>(&B.ldt[lane], I.ldt + id);
                 async_copy<8>(&B.ivm[lane], I.inv_vol + id);
                 if (LAST) async_copy<sizeof(T)>(&B.volm[lane], I.mg + MG_N * (id + nj) + MG_VOL);
@@ -536,12 +547,19 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     double sc = a * (PIPE ? B->ivm[lane] : ld(I.inv_vol + id));
                     double un[5], uo0 = 0.0;
                     for (int v = 0; v < 5; ++v) {
-                        double uo = PIPE ? B->un[v][lane] : I.un[v][id];
-                        if (v == 0) uo0 = uo;
-                        if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
-                        else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
-                        dst[v][id] = (TD)un[v];
-                        if (LAST && sizeof(T) != sizeof(double)) I.uc[v][id] = (T)un[v];
+                        if constexpr (ACC32) {
+                            T a0 = FIRST ? UA(1, v) : (PIPE ? B->uacc[v][lane] : ld(I.uc[v] + id));
+                            T nv = a0 - R[v] * (T)sc;
+                            un[v] = (double)nv;
+                            dst[v][id] = (TD)nv;
+                        } else {
+                            double uo = PIPE ? B->un[v][lane] : I.un[v][id];
+                            if (v == 0) uo0 = uo;
+                            if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
+                            else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
+                            dst[v][id] = (TD)un[v];
+                            if (LAST && sizeof(T) != sizeof(double)) I.uc[v][id] = (T)un[v];
+                        }
                     }
                     // unpack checks (solver.rs:160-171), on the stored precision
                     bool bad;
