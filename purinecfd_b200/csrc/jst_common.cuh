@@ -203,12 +203,31 @@ template <class T> JST_HD T fw_of(T r, T cw2, T cw3_6, T one_plus_cw3_6) {
 // reference formula would give inf * 0 = NaN, where FP64 still evaluates it
 // (to (1 + Cw3^6)^(1/6) within rounding once g^6 dwarfs Cw3^6).  So g is
 // formed in FP64 and, beyond g = 1e5, fw takes that limit.
+// The sixth root is taken as 2^(log2(x) / 6) with the hardware base-2
+// logarithm and exponential (x > 0 here); in FP32 that is accurate to a few
+// units in the last place, against the two library roots sqrt and cbrt.
+JST_HD float root6_f32(float x) {
+#ifdef __CUDA_ARCH__
+    return exp2f(__log2f(x) * (1.0f / 6.0f));
+#else
+    return std::exp2(std::log2(x) * (1.0f / 6.0f));
+#endif
+}
+
+JST_HD float exp_f32(float x) {
+#ifdef __CUDA_ARCH__
+    return __expf(x);
+#else
+    return std::exp(x);
+#endif
+}
+
 JST_HD float fw_of_f32(float r, double cw2, double cw3_6, double one_plus_cw3_6, double fw_lim) {
     double rd = (double)r;
     double g = rd + cw2 * (powi6<double>(rd) - rd);
     if (g > 1e5) return (float)fw_lim;
     float gf = (float)g;
-    return gf * cbrt(sqrt((float)one_plus_cw3_6 / (powi6<float>(gf) + (float)cw3_6)));
+    return gf * root6_f32((float)one_plus_cw3_6 / (powi6<float>(gf) + (float)cw3_6));
 }
 
 // source::compute for one cell (source.rs:55-85), before the factor V.
@@ -216,7 +235,9 @@ template <class T>
 JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny, const PhysConst& c) {
     T nu_tilde = rho_nu / rho;
     T inv_kd2 = inv_dist2 * T(c.inv_kappa2);
-    T ft2 = T(c.Ct3) * exp(-T(c.Ct4) * chi * chi);
+    T ft2;
+    if constexpr (sizeof(T) == sizeof(float)) ft2 = T(c.Ct3) * exp_f32(-T(c.Ct4) * chi * chi);
+    else ft2 = T(c.Ct3) * exp(-T(c.Ct4) * chi * chi);
     T fv2 = T(1) - chi / (T(1) + chi * f1);
     T sv = T(c.fv3) * fabs(dvdx - dudy);
     T s_tilde = tmax<T>(sv + nu_tilde * inv_kd2 * fv2, T(1e-10));
