@@ -229,10 +229,17 @@ void default_tile(int prec, int nj, int* ti, int* tj) {
 }
 
 // Tile configurations the autotuner times, in order (TI, TJ, threads).
-// Marching candidates are (maximum strip height, 26, threads).
-const int kTileCands[][3] = {{8, 32, 256}, {8, 32, 192}, {16, 32, 384}, {16, 32, 256}, {4, 32, 256},
-                             {4, 64, 256},  {8, 64, 256}, {8, 32, 128}, {16, 26, 64},  {24, 26, 64},
-                             {32, 26, 64},  {48, 26, 64}, {64, 26, 64}, {32, 26, 128}};
+// Marching candidates are (maximum strip height, 26, threads); the tile
+// configurations kept here are the ones that were ever fastest on some mesh.
+const int kTileCands[][3] = {{4, 32, 256}, {8, 32, 256}, {16, 32, 256}, {16, 26, 64},
+                             {32, 26, 64}, {48, 26, 64}, {64, 26, 64},  {32, 26, 128}};
+
+// Below this many cells the autotuner times a short list: on small meshes a
+// stage is latency-bound and small tiles win (the marching kernel's row walk
+// cannot be hidden behind other strips), and the first use of every
+// candidate's kernels costs more than a small solve.
+constexpr long kTuneMinCells = 262144;
+const int kSmallCands[][3] = {{4, 32, 256}, {8, 32, 256}, {16, 32, 256}};
 
 // Stage input buffer = T copy of U_n, so a middle stage can be timed without
 // touching the solution.
@@ -267,6 +274,7 @@ std::vector<TileRef> make_tiles(int inst, int ni, int nj, int ti, int tj) {
 int tuned_tiles_bound(int ni, int nj) {
     int m = ((ni + 7) / 8) * ((nj + fused::MARCH_W - 1) / fused::MARCH_W);
     for (const auto& cd : kTileCands) m = std::max(m, ((ni + cd[0] - 1) / cd[0]) * ((nj + cd[1] - 1) / cd[1]));
+    for (const auto& cd : kSmallCands) m = std::max(m, ((ni + cd[0] - 1) / cd[0]) * ((nj + cd[1] - 1) / cd[1]));
     return m;
 }
 
@@ -297,6 +305,28 @@ int march_height(const std::vector<std::pair<int, std::pair<int, int>>>& insts, 
     return best_h;
 }
 
+// The marching configuration the wave model picks for the given instances
+// (64 threads per block), without timing anything.
+template <class T> TuneResult model_choice(const std::vector<std::pair<int, std::pair<int, int>>>& insts) {
+    TuneResult r{32, fused::MARCH_W, 64, 0.f};
+    Kernels<T> K;
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (pick_kernels<T>(32, fused::MARCH_W, &K, 64) &&
+        cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K.stage[1], K.nt, K.smem) == cudaSuccess)
+        r.ti = march_height(insts, (long)sms * std::max(1, occ) * (K.nt / 32));
+    cudaGetLastError();
+    return r;
+}
+
+long total_cells(const std::vector<std::pair<int, std::pair<int, int>>>& insts) {
+    long n = 0;
+    for (const auto& in : insts) n += (long)in.second.first * in.second.second;
+    return n;
+}
+
 // Times one middle-stage launch per candidate over the given instances
 // (their U_a must hold a valid state) and returns the fastest configuration.
 template <class T>
@@ -313,18 +343,14 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     std::vector<std::array<int, 3>> cands;
-    for (const auto& cd : kTileCands) cands.push_back({cd[0], cd[1], cd[2]});
-    {
-        Kernels<T> K;
-        int occ = 1;
-        if (pick_kernels<T>(32, fused::MARCH_W, &K, 64) &&
-            cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K.stage[1], K.nt, K.smem) == cudaSuccess) {
-            int h = march_height(insts, (long)sms * occ * (K.nt / 32));
-            cands.push_back({h, fused::MARCH_W, 64});
-            cands.push_back({h, fused::MARCH_W, 128});
-        }
-        cudaGetLastError();
+    const TuneResult m = model_choice<T>(insts);
+    if (total_cells(insts) < kTuneMinCells) {
+        for (const auto& cd : kSmallCands) cands.push_back({cd[0], cd[1], cd[2]});
+        cands.push_back({m.ti, m.tj, 64});
+    } else {
+        for (const auto& cd : kTileCands) cands.push_back({cd[0], cd[1], cd[2]});
+        cands.push_back({m.ti, m.tj, 64});
+        cands.push_back({m.ti, m.tj, 128});
     }
     for (const auto& cand : cands) {
         Kernels<T> K;
@@ -1085,12 +1111,12 @@ template <class T> class Batch : public BatchBase {
         tune_ = false;
         std::vector<std::pair<int, std::pair<int, int>>> list;
         for (int k = 0; k < nslots_; ++k)
-            if (slots_[k].used) {
-                list.push_back({k, {slots_[k].ni, slots_[k].nj}});
-                long n = (long)slots_[k].ni * slots_[k].nj;
-                JST_LAUNCH(k_copy_state<T>, (unsigned)((n + 255) / 256), 256, 0, st_, h_insts_[k], n);
-            }
+            if (slots_[k].used) list.push_back({k, {slots_[k].ni, slots_[k].nj}});
         if (list.empty()) return;
+        for (const auto& in : list) {
+            long n = (long)in.second.first * in.second.second;
+            JST_LAUNCH(k_copy_state<T>, (unsigned)((n + 255) / 256), 256, 0, st_, h_insts_[in.first], n);
+        }
         TuneResult r = autotune<T>(list, d_insts_, d_states_, nslots_, st_, 1);
         if (!select_kernels(r.ti, r.tj, r.nt)) return;
         h_tiles_.clear();
