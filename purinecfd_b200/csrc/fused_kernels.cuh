@@ -74,7 +74,8 @@ template <class T> struct Inst {
     // geometry, FP64 (geometry.rs:45-63)
     const double *tnx, *tny, *nnx, *nny, *vol, *inv_vol, *inv_d2;
     const double* far;  // per column j: tau(NI) normal x,y and centroid distances of cells NI-1..NI-3 (5*nj)
-    // state
+    // state; the five planes of each array are contiguous (plane k at plane 0
+    // + k * ni * nj), which the marching kernel relies on
     double* un[5];      // U_n, the FP64 step-start state
     T* ua[5];           // stage ping-pong buffers
     T* ub[5];

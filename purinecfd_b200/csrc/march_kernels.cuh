@@ -200,14 +200,13 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         const T* ratio = I.ratio[step & 1];
         T* ratio_next = I.ratio[(step + 1) & 1];
         (void)ratio_next;
-        const T* src[5];
-        TD* dst[5];
-        for (int v = 0; v < 5; ++v) {
-            if (FIRST) src[v] = sizeof(T) == sizeof(double) ? reinterpret_cast<const T*>(I.un[v]) : I.uc[v];
-            else src[v] = (stage % 2 == 1) ? I.ua[v] : I.ub[v];
-            if (LAST) dst[v] = reinterpret_cast<TD*>(I.un[v]);
-            else dst[v] = reinterpret_cast<TD*>((stage % 2 == 0) ? I.ua[v] : I.ub[v]);
-        }
+        // The five planes of every state array are contiguous (plane k at
+        // plane 0 + k * NI * NJ, as both engines allocate them), so one base
+        // pointer per array and the plane stride address them all.
+        const long np = (long)ni * nj;
+        const T* src = FIRST ? (sizeof(T) == sizeof(double) ? reinterpret_cast<const T*>(I.un[0]) : I.uc[0])
+                             : ((stage % 2 == 1) ? I.ua[0] : I.ub[0]);
+        TD* dst = LAST ? reinterpret_cast<TD*>(I.un[0]) : reinterpret_cast<TD*>((stage % 2 == 0) ? I.ua[0] : I.ub[0]);
 
         const int i1 = tr.i1;                       // output rows i0 .. i1-1
         const int cu = j0 - 3 + lane;               // unwrapped column of this lane
@@ -225,7 +224,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             MarchRow<T>& B = rowbuf[kk & 1];
             if (S || kk < ni) {
                 const long id = (long)(kk < 0 ? -1 - kk : kk) * nj + gj;
-                for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.u[v][lane], src[v] + id);
+                for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.u[v][lane], src + v * np + id);
             }
             if (S || (kk >= 0 && kk <= ni)) {
                 const T* g = I.mg + MG_N * ((long)kk * nj + gj);
@@ -242,9 +241,9 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 const long id = (long)m * nj + gj;
                 if constexpr (ACC32) {
                     if constexpr (!FIRST)  // stage 0 reads the same values as its stage input
-                        for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.uacc[v][lane], I.uc[v] + id);
+                        for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.uacc[v][lane], I.uc[0] + v * np + id);
                 } else {
-                    for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[v] + id);
+                    for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[0] + v * np + id);
                 }
                 if (I.local_dt) async_copy<8>(&B.ldt[lane], I.ldt + id);
                 async_copy<8>(&B.ivm[lane], I.inv_vol + id);
@@ -315,7 +314,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 const bool wall = !S && k < 0;
                 const int kr = wall ? -1 - k : k;  // the wall ghost mirrors cell -1-k (boundary.rs:30-51)
                 const long id = (long)kr * nj + gj;
-                for (int v = 0; v < 5; ++v) uk[v] = PIPE ? B->u[v][lane] : ld(src[v] + id);
+                for (int v = 0; v < 5; ++v) uk[v] = PIPE ? B->u[v][lane] : ld(src + v * np + id);
                 Prim<T> p;
                 if (fresh) {
                     p.rho = (T)c.f_rho;
@@ -548,17 +547,17 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     double un[5], uo0 = 0.0;
                     for (int v = 0; v < 5; ++v) {
                         if constexpr (ACC32) {
-                            T a0 = FIRST ? UA(1, v) : (PIPE ? B->uacc[v][lane] : ld(I.uc[v] + id));
+                            T a0 = FIRST ? UA(1, v) : (PIPE ? B->uacc[v][lane] : ld(I.uc[0] + v * np + id));
                             T nv = a0 - R[v] * (T)sc;
                             un[v] = (double)nv;
-                            dst[v][id] = (TD)nv;
+                            dst[v * np + id] = (TD)nv;
                         } else {
-                            double uo = PIPE ? B->un[v][lane] : I.un[v][id];
+                            double uo = PIPE ? B->un[v][lane] : I.un[0][v * np + id];
                             if (v == 0) uo0 = uo;
                             if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
                             else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
-                            dst[v][id] = (TD)un[v];
-                            if (LAST && sizeof(T) != sizeof(double)) I.uc[v][id] = (T)un[v];
+                            dst[v * np + id] = (TD)un[v];
+                            if (LAST && sizeof(T) != sizeof(double)) I.uc[0][v * np + id] = (T)un[v];
                         }
                     }
                     // unpack checks (solver.rs:160-171), on the stored precision
