@@ -105,6 +105,41 @@ __global__ void k_geom_wall(Geom g, int window) {
     g.inv_d2[id] = 1.0 / (best * best);
 }
 
+// The same wall distance, one block per (row i, 256 consecutive columns): the
+// block's window of wall midpoints is staged in shared memory once, and since
+// sqrt is monotonic and correctly rounded, sqrt(min d^2) is the reference's
+// min sqrt(d^2) bit for bit, with one square root per cell.
+constexpr int kWallBlock = 256;
+constexpr size_t kWallSmemMax = 200 * 1024;
+
+__global__ void __launch_bounds__(kWallBlock) k_geom_wall_rows(Geom g, int window) {
+    extern __shared__ double wm[];  // x then y of faces j0-window .. j0+kWallBlock-1+window
+    const int L = 2 * window + kWallBlock;
+    double* sx = wm;
+    double* sy = wm + L;
+    const long nj = g.nj;
+    const long j0 = (long)blockIdx.x * kWallBlock;
+    for (int e = threadIdx.x; e < L; e += kWallBlock) {
+        long k = ((j0 - window + e) % nj + nj) % nj;  // geometry.rs:206 rem_euclid
+        sx[e] = g.tmx[k];
+        sy[e] = g.tmy[k];
+    }
+    __syncthreads();
+    const long j = j0 + threadIdx.x;
+    if (j >= nj) return;
+    const long id = (long)blockIdx.y * nj + j;
+    const double px = g.cx[id], py = g.cy[id];
+    double best2 = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+    for (int e = threadIdx.x; e <= threadIdx.x + 2 * window; ++e) {
+        double ex = px - sx[e], ey = py - sy[e];
+        double d2 = powi2(ex) + powi2(ey);
+        if (d2 < best2) best2 = d2;
+    }
+    const double best = sqrt(best2);
+    g.wdist[id] = best;
+    g.inv_d2[id] = 1.0 / (best * best);
+}
+
 // ------------------------------------------------------------ passes path --
 struct DF {
     double* p;
@@ -629,7 +664,15 @@ void geometry_build(const double* d_xy, int n_rings, int n_theta, Geom& g, cudaS
     JST_LAUNCH(k_geom_faces, nblk(nt + n), TB, 0, st, m, g);
     long nj = g.nj;
     int window = (int)std::min(std::max(15L, nj / 5), nj / 2);
-    JST_LAUNCH(k_geom_wall, nblk(n), TB, 0, st, g, window);
+    size_t smem = 2 * (size_t)(2 * window + kWallBlock) * sizeof(double);
+    if (smem <= kWallSmemMax && g.ni <= 65535 &&
+        cudaFuncSetAttribute(k_geom_wall_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess) {
+        dim3 grid((unsigned)((nj + kWallBlock - 1) / kWallBlock), (unsigned)g.ni);
+        k_geom_wall_rows<<<grid, kWallBlock, smem, st>>>(g, window);
+    } else {
+        cudaGetLastError();
+        JST_LAUNCH(k_geom_wall, nblk(n), TB, 0, st, g, window);
+    }
 }
 
 struct Passes {

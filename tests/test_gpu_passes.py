@@ -6,7 +6,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import cmp_field, golden_cases, load_golden
+from conftest import cmp_field, golden_cases, load_config, load_golden
 from gpu_common import STATE_FIELDS, cylinder_case, mesh_case, rel_field_err
 
 import jst_oracle as jo
@@ -36,6 +36,26 @@ def test_geometry_bit_exact(golden):
         assert np.array_equal(s.get(name), o.get(name)), name
     for which in (0, 1):
         assert np.array_equal(s.faces(which).ravel(), o.faces(which)), which
+
+
+@pytest.mark.parametrize("mesh", ["naca_129x256", "naca_257x512", "ellipse_29x70", "cylinder_65x300"])
+def test_wall_distance_bit_exact_on_larger_meshes(mesh):
+    """The GPU wall distance (a shared-memory window per block, one square
+    root per cell) equals the reference's per-face search bit for bit, on
+    rings wider and narrower than a block and with windows up to nj/5."""
+    from purinecfd_b200 import Solver, meshgen
+    kind, size = mesh.split("_")
+    nr, nt = map(int, size.split("x"))
+    if kind == "naca":
+        xy = meshgen.naca4_o_mesh(nr, nt, 0.02, 0.4, 0.12, first_spacing=1e-6)
+    elif kind == "ellipse":
+        xy = meshgen.ellipse_o_mesh(nr, nt, stretch=1.1)
+    else:
+        xy = meshgen.cylinder_o_mesh(nr, nt, radius=0.5, r_far=20.0, first_spacing=1e-3)
+    cfg = load_config()
+    s = Solver(cfg, xy, nr, nt)
+    o = jo.OracleSolver(cfg, xy, nr, nt)
+    assert np.array_equal(s.get("wall_dist"), o.get("wall_dist"))
 
 
 def test_initial_state_bit_exact(golden):
