@@ -548,7 +548,7 @@ template <class T> class FusedEngine : public Engine {
         cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_ntiles_, &ntiles_, sizeof(int), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_unptr_, inst_.un, 5 * sizeof(double*), cudaMemcpyHostToDevice, C.st);
-        if (cudaMallocHost(&h_state_, sizeof(InstState)) != cudaSuccess) {
+        if (cudaMallocHost(&h_state_, 3 * sizeof(InstState)) != cudaSuccess) {
             err = "cudaMallocHost failed";
             return false;
         }
@@ -718,8 +718,9 @@ template <class T> class FusedEngine : public Engine {
         int64_t cap = std::min<int64_t>(limit, INT_MAX - 1 - start);
         if ((size_t)(start + cap) > hist_cap_) grow_hist((size_t)(start + cap));
         set_max_step((int)(start + cap));
+        if (cb) return run_with_callback(start, cap, cb, user, done, res, bad);
         int64_t queued = 0;
-        const int64_t chunk = cb ? 1 : 64;
+        const int64_t chunk = 64;
         int reported = start;
         while (queued < cap) {
             int64_t nq = std::min(chunk, cap - queued);
@@ -737,6 +738,50 @@ template <class T> class FusedEngine : public Engine {
         *done = s.step - start;
         *res = s.step > start ? s.residual : std::numeric_limits<double>::quiet_NaN();
         if (s.bad != fused::NO_BAD) return report(s.bad, bad);
+        return JST_OK;
+    }
+
+    // The run loop with a per-step callback: one RK step stays queued ahead of
+    // the host, which reads the previous step's scalars from pinned memory
+    // (copied on the stream right after that step) and calls back in order;
+    // a step queued past convergence, NonPhysical or the limit is skipped on
+    // the device.
+    jst_status run_with_callback(int start, int64_t cap, jst_step_cb cb, void* user, int64_t* done, double* res,
+                                 jst_nonphysical* bad) {
+        cudaStream_t st = core_->st;
+        InstState* slot[2] = {h_state_ + 1, h_state_ + 2};
+        cudaEvent_t ev[2];
+        for (auto& e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        auto enqueue = [&](int64_t q) {
+            launch_step();
+            cudaMemcpyAsync(slot[q & 1], inst_.st, sizeof(InstState), cudaMemcpyDeviceToHost, st);
+            cudaEventRecord(ev[q & 1], st);
+        };
+        jst_status rc = JST_OK;
+        int64_t queued = 0;
+        int reported = start;
+        InstState s{};
+        enqueue(queued++);
+        for (int64_t q = 0; q < cap; ++q) {
+            if (queued < cap) enqueue(queued++);
+            if (cudaEventSynchronize(ev[q & 1]) != cudaSuccess) {
+                rc = JST_ERR_CUDA;
+                break;
+            }
+            s = *slot[q & 1];
+            if (s.step > reported) {
+                reported = s.step;
+                cb(user, (uint64_t)(reported - start), s.residual);
+            }
+            if (s.bad != fused::NO_BAD || s.done || s.step >= start + cap) break;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        InstState fin;
+        if (read_state(&fin) != JST_OK) return JST_ERR_CUDA;  // also waits for a step queued ahead
+        if (rc != JST_OK) return rc;
+        *done = fin.step - start;
+        *res = fin.step > start ? fin.residual : std::numeric_limits<double>::quiet_NaN();
+        if (fin.bad != fused::NO_BAD) return report(fin.bad, bad);
         return JST_OK;
     }
 

@@ -196,6 +196,11 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         if (skip) continue;
         const int fresh = jst_shfl_idx(hdr[1], 0);
         const int step = jst_shfl_idx(hdr[2], 0);
+        // per-instance values the row walk uses, read once per strip (the step's
+        // global time step changes only when the last strip of the last stage
+        // has finished)
+        const bool dt_local = I.local_dt != 0;
+        const double adt = dt_local ? alpha : alpha * I.st->dt;
         const unsigned long long stage_id = (unsigned long long)step * 5 + stage;
         const T* ratio = I.ratio[step & 1];
         T* ratio_next = I.ratio[(step + 1) & 1];
@@ -245,7 +250,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 } else {
                     for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[0] + v * np + id);
                 }
-                if (I.local_dt) async_copy<8>(&B.ldt[lane], I.ldt + id);
+                if (dt_local) async_copy<8>(&B.ldt[lane], I.ldt + id);
                 async_copy<8>(&B.ivm[lane], I.inv_vol + id);
                 if (LAST) async_copy<sizeof(T)>(&B.volm[lane], I.mg + MG_N * (id + nj) + MG_VOL);
             }
@@ -542,7 +547,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     T R[5];
                     for (int v = 0; v < 5; ++v) R[v] = (ftn[v] - ft[v]) + (fnr[v] - fn[v]);
                     R[4] -= sw[0];
-                    double a = alpha * (I.local_dt ? (PIPE ? B->ldt[lane] : ld(I.ldt + id)) : I.st->dt);
+                    double a = dt_local ? alpha * (PIPE ? B->ldt[lane] : ld(I.ldt + id)) : adt;
                     double sc = a * (PIPE ? B->ivm[lane] : ld(I.inv_vol + id));
                     double un[5], uo0 = 0.0;
                     for (int v = 0; v < 5; ++v) {
@@ -595,7 +600,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
                         T dl = local_dt<T>(qvx, qvy, sqrt((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
                         ratio_next[id] = vol / dl;
-                        if (I.local_dt) I.ldt[id] = (double)dl;
+                        if (dt_local) I.ldt[id] = (double)dl;
                         mloc = fmin(mloc, (double)dl);
                     }
                 }
