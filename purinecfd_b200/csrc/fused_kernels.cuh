@@ -351,6 +351,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
     double* red = reinterpret_cast<double*>(smem_raw + L::red_off);
     double* farbuf = red + NT;  // 7 values per staged column of a far-field tile
     __shared__ int flags[4];
+    __shared__ double adt_s;
     const int nt_all = *ntiles;
     // Persistent over the tile table: blocks stride through (instance, tile) items.
     for (int tix = JST_BID(); tix < nt_all; tix += (int)JST_GRID()) {
@@ -369,6 +370,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
         flags[0] = skip;
         flags[1] = FIRST ? st->fresh : 0;
         flags[2] = step;
+        adt_s = alpha * st->dt;  // the step's global time step, read once per tile
         if (FIRST && !skip && tr.tile == 0) st->totaltime += st->dt;
     }
     JST_SYNC();
@@ -723,7 +725,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
             R[k] = (sFt[k * L::NFT + w + TJ] - sFt[k * L::NFT + w]) + (sFn[k * L::NFN + fd + 1] - sFn[k * L::NFN + fd]);
         R[4] -= sS[w];
         int rc = (ti + 1) * RJ + tj + 1;  // ring index of the cell
-        double a = alpha * (I.local_dt ? ld(I.ldt + id) : I.st->dt);
+        double a = I.local_dt ? alpha * ld(I.ldt + id) : adt_s;
         double sc = a * gs[L::gIV + rc];
         double un[5];
         for (int k = 0; k < 5; ++k) {
