@@ -360,7 +360,10 @@ def batched_leg(args, world: int = 1, rank: int = 0):
         cases.append((cfg, xy, nr, nt))
     part = {"instances": len(cases), "cells": sum((c[2] - 1) * c[3] for c in cases)}
     barrier(world)
-    split, part["wall_split"] = batch_solve(cases, PREC_FP32_SPLIT, max_steps=args.batch_steps) if cases else ([], 0.0)
+    kinfo = {}
+    split, part["wall_split"] = (batch_solve(cases, PREC_FP32_SPLIT, max_steps=args.batch_steps, info=kinfo)
+                                 if cases else ([], 0.0))
+    part["kernel"] = kinfo.get("kernel")
     barrier(world)
     ref, part["wall_ref"] = batch_solve(cases, PREC_FP64, max_steps=args.batch_steps) if cases else ([], 0.0)
     part["plain_m"], part["plain_wall"] = 0, 0.0
@@ -404,6 +407,7 @@ def combine_batch_parts(parts: list, step_cap: int) -> dict:
     errs = [p["dcl_max"] for p in parts if p["dcl_max"] is not None]
     errd = [p["dcd_max"] for p in parts if p["dcd_max"] is not None]
     out = {"instances": n, "ranks": world, "cells": sum(p["cells"] for p in parts), "step_cap": step_cap,
+           "kernel": parts[0].get("kernel"),
            "solves_per_s": round(n / wall, 3) if wall > 0 else None, "wall_s": round(wall, 3),
            "mcell_stage_per_s": round(sum(p["cell_steps"] for p in parts) * 5 / wall / 1e6, 1) if wall > 0 else None,
            "p50_s": round(percentile(lat, 50), 3), "p99_s": round(percentile(lat, 99), 3),

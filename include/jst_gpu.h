@@ -247,6 +247,11 @@ jst_status jst_batch_submit(jst_batch* b, const char* config_json, const double*
  * after nsteps or when nothing is active or queued. */
 jst_status jst_batch_step(jst_batch* b, int nsteps);
 
+/* (tile_i, tile_j, block_threads) the batch's stage kernel runs with: set by
+ * the options or, when those are 0, by the autotuner at the first
+ * jst_batch_step (tile_j == 26: marching strips of at most tile_i rows). */
+jst_status jst_batch_kernel_config(const jst_batch* b, int* tile_i, int* tile_j, int* block_threads);
+
 /* Counts of active and queued instances and device bytes in use. */
 jst_status jst_batch_stats(jst_batch* b, int* active, int* queued, double* bytes_in_use);
 

@@ -52,6 +52,12 @@ class BatchResult:
         return self.t_done - self.t_submit
 
 
+# The batch entry points of include/jst_gpu.h this module binds.
+BATCH_EXPORTS = ["jst_batch_default_opts", "jst_batch_create", "jst_batch_destroy", "jst_batch_submit",
+                 "jst_batch_step", "jst_batch_stats", "jst_batch_poll", "jst_batch_result_get",
+                 "jst_batch_kernel_config"]
+
+
 def _bind():
     L = lib()
     if getattr(L, "_batch_bound", False):
@@ -64,6 +70,7 @@ def _bind():
     L.jst_batch_submit.argtypes = [vp, C.c_char_p, pd, i, i, C.c_int64, d, d, C.POINTER(C.c_int64)]
     L.jst_batch_step.argtypes = [vp, i]
     L.jst_batch_stats.argtypes = [vp, C.POINTER(i), C.POINTER(i), pd]
+    L.jst_batch_kernel_config.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     L.jst_batch_poll.argtypes = [vp, C.POINTER(C.c_int64), i, C.POINTER(i)]
     L.jst_batch_result_get.argtypes = [vp, C.c_int64, C.POINTER(BatchResultC), pd, C.c_size_t]
     L._batch_bound = True
@@ -120,6 +127,12 @@ class Batch:
         a, q, b = C.c_int(), C.c_int(), C.c_double()
         lib().jst_batch_stats(self._h, C.byref(a), C.byref(q), C.byref(b))
         return a.value, q.value, b.value
+
+    def kernel_config(self):
+        """(tile_i, tile_j, block_threads) of the batch's stage kernel."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        lib().jst_batch_kernel_config(self._h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
 
     def poll(self, cap: int = 4096) -> list[int]:
         ids = (C.c_int64 * cap)()

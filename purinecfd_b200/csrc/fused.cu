@@ -1040,6 +1040,7 @@ class BatchBase {
     virtual void stats(int* active, int* queued, double* bytes) = 0;
     virtual int poll(int64_t* ids, int cap) = 0;
     virtual bool result(int64_t id, BatchResultFull** out) = 0;
+    virtual void kernel_config(int* ti, int* tj, int* nt) const = 0;
 };
 
 template <class T> class Batch : public BatchBase {
@@ -1535,6 +1536,12 @@ template <class T> class Batch : public BatchBase {
         return JST_OK;
     }
 
+    void kernel_config(int* ti, int* tj, int* nt) const override {
+        *ti = ti_;
+        *tj = tj_;
+        *nt = K_.nt;
+    }
+
     void stats(int* a, int* q, double* bytes) override {
         if (a) *a = active_;
         if (q) *q = (int)queue_.size();
@@ -1633,6 +1640,12 @@ jst_status jst_batch_submit(jst_batch* b, const char* cfg, const double* xy, int
 }
 
 jst_status jst_batch_step(jst_batch* b, int nsteps) { return b ? b->impl->step(nsteps) : JST_ERR_ARG; }
+
+jst_status jst_batch_kernel_config(const jst_batch* b, int* ti, int* tj, int* nt) {
+    if (!b || !ti || !tj || !nt) return JST_ERR_ARG;
+    b->impl->kernel_config(ti, tj, nt);
+    return JST_OK;
+}
 
 jst_status jst_batch_stats(jst_batch* b, int* active, int* queued, double* bytes) {
     if (!b) return JST_ERR_ARG;

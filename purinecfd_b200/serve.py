@@ -111,15 +111,18 @@ def serve(requests: list[Request], rate: float, seed: int = 0, precision: int = 
 
 
 def batch_solve(cases, precision: int, max_instances: int = 256, max_steps: int = 2000, residual_drop: float = 1e-6,
-                cl_tol: float = 0.0, hbm_budget_gb: float = 40.0, steps_per_poll: int = 25):
+                cl_tol: float = 0.0, hbm_budget_gb: float = 40.0, steps_per_poll: int = 25, info: dict | None = None):
     """Solve every case (config, xy, n_rings, n_theta) in one batch; returns
-    (results in case order, wall seconds)."""
+    (results in case order, wall seconds).  `info`, when given, receives the
+    stage kernel configuration the batch ran with."""
     b = Batch(precision=precision, dt_mode=DT_LOCAL, steps_per_poll=steps_per_poll, hbm_budget_gb=hbm_budget_gb,
               max_instances=max_instances)
     t0 = time.perf_counter()
     ids = [b.submit(c[0], c[1], c[2], c[3], max_steps, residual_drop, cl_tol) for c in cases]
     res = {r.id: r for r in b.run_all(chunk=max(steps_per_poll, 100))}
     wall = time.perf_counter() - t0
+    if info is not None:
+        info["kernel"] = "x".join(map(str, b.kernel_config()))
     b.close()
     return [res[i] for i in ids], wall
 

@@ -91,3 +91,19 @@ def test_admission_is_limited_by_slots_and_continues():
     assert a <= 2 and a + q == 5
     res = {r.id: r for r in b.run_all(chunk=30)}
     assert set(res) == set(ids) and all(r.steps == 30 for r in res.values())
+
+
+def test_kernel_configuration_is_reported():
+    """Given options are kept; otherwise the autotuner's choice at the first
+    step is one of the compiled configurations."""
+    from purinecfd_b200.batch import Batch
+    cases = _cases()
+    fixed = Batch(tile_i=32, tile_j=26, block_threads=64, steps_per_poll=10, hbm_budget_gb=1.0)
+    fixed.submit(*cases[0], max_steps=10)
+    fixed.run_all(chunk=10)
+    assert fixed.kernel_config() == (32, 26, 64)
+    tuned = Batch(steps_per_poll=10, hbm_budget_gb=1.0)
+    tuned.submit(*cases[1], max_steps=10)
+    tuned.run_all(chunk=10)
+    ti, tj, nt = tuned.kernel_config()
+    assert tj in (26, 32, 64) and ti > 0 and nt in (64, 128, 256)
