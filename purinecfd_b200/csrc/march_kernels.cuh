@@ -35,6 +35,90 @@ namespace fused {
 
 constexpr int MARCH_W = 26;  // output columns per strip (32 lanes - 2 x 3 halo)
 
+// Paired FP32 arithmetic (sm_100 f32x2 instructions: one instruction for two
+// lanes of data) for the five-component face arithmetic, where components
+// (1, 2) and (3, 4) go in pairs and component 0 alone.  A pair lives in one
+// 64-bit register (hand-written PTX); the emulation build does it per lane.
+#ifdef __CUDA_ARCH__
+using f2 = unsigned long long;
+JST_D f2 f2_make(float a, float b) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+JST_D void f2_split(f2 r, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r)); }
+JST_D f2 f2_fma(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+JST_D f2 f2_add(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+JST_D f2 f2_mul(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+#else
+struct f2 {
+    float x, y;
+};
+JST_D f2 f2_make(float a, float b) { return f2{a, b}; }
+JST_D void f2_split(f2 r, float& a, float& b) {
+    a = r.x;
+    b = r.y;
+}
+JST_D f2 f2_fma(f2 a, f2 b, f2 c) { return f2{fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y)}; }
+JST_D f2 f2_add(f2 a, f2 b) { return f2{a.x + b.x, a.y + b.y}; }
+JST_D f2 f2_mul(f2 a, f2 b) { return f2{a.x * b.x, a.y * b.y}; }
+#endif
+JST_D f2 f2_splat(float a) { return f2_make(a, a); }
+
+// Net face flux out = cv - vis - lam (d1 e2 - d3 e4) of the five components,
+// with d1 = w2 - w1 and d3 = w3 - 3 w2 + 3 w1 - w0 (w0..w3 the states at
+// face-2 .. face+1) and vis = (dA + dB) hx + (dA' + dB') hy from the two
+// cells' diffusion tensors (components 1-4; component 0 has none).
+template <class T>
+JST_D void face_combine(const T* w0, const T* w1, const T* w2, const T* w3, const T* cv, const T* dA, const T* dB,
+                        T hx, T hy, T lam, T e2, T e4, T* out) {
+    if constexpr (sizeof(T) == sizeof(float)) {
+        {  // component 0
+            T d1 = w2[0] - w1[0];
+            T d3 = w3[0] - T(3) * w2[0] + T(3) * w1[0] - w0[0];
+            out[0] = cv[0] - lam * (d1 * e2 - d3 * e4);
+        }
+        const f2 m1 = f2_splat(-1.0f), m3 = f2_splat(-3.0f), p3 = f2_splat(3.0f);
+        const f2 hx2 = f2_splat(hx), hy2 = f2_splat(hy), e22 = f2_splat(e2), me42 = f2_splat(-e4);
+        const f2 mlam = f2_splat(-lam);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int a = 1 + 2 * q, b = a + 1;  // components a, b; tensor rows a-1, b-1 (x) and a+3, b+3 (y)
+            f2 W0 = f2_make(w0[a], w0[b]), W1 = f2_make(w1[a], w1[b]), W2 = f2_make(w2[a], w2[b]);
+            f2 W3 = f2_make(w3[a], w3[b]);
+            f2 D1 = f2_fma(W1, m1, W2);
+            f2 D3 = f2_fma(W0, m1, f2_fma(W1, p3, f2_fma(W2, m3, W3)));
+            f2 DX = f2_add(f2_make(dA[a - 1], dA[b - 1]), f2_make(dB[a - 1], dB[b - 1]));
+            f2 DY = f2_add(f2_make(dA[a + 3], dA[b + 3]), f2_make(dB[a + 3], dB[b + 3]));
+            f2 VIS = f2_fma(DX, hx2, f2_mul(DY, hy2));
+            f2 DIS = f2_fma(D3, me42, f2_mul(D1, e22));
+            f2 O = f2_fma(DIS, mlam, f2_fma(VIS, m1, f2_make(cv[a], cv[b])));
+            f2_split(O, out[a], out[b]);
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            T d1 = w2[v] - w1[v];
+            T d3 = w3[v] - T(3) * w2[v] + T(3) * w1[v] - w0[v];
+            T vis = T(0);
+            if (v > 0) vis = (dA[v - 1] + dB[v - 1]) * hx + (dA[v + 3] + dB[v + 3]) * hy;
+            out[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
+        }
+    }
+}
+
 template <class V> JST_D V warp_sum0(V v) {  // lane 0 gets a fixed-order sum
     for (int o = 16; o > 0; o >>= 1) v += jst_shfl_xor(v, o);
     return v;
@@ -495,13 +579,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 const T fnx = tx[1], fny = ty[1];
                 euler_flux<T>(fu, fnx, fny, gm1, cv, p_ref);
                 T hx = T(0.5) * fnx, hy = T(0.5) * fny;
-                for (int v = 0; v < 5; ++v) {
-                    T d1 = w2[v] - w1[v];
-                    T d3 = w3[v] - T(3) * w2[v] + T(3) * w1[v] - w0[v];
-                    T vis = T(0);
-                    if (v > 0) vis = (dw[0][v - 1] + dw[1][v - 1]) * hx + (dw[0][v + 3] + dw[1][v + 3]) * hy;
-                    ftn[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
-                }
+                face_combine<T>(w0, w1, w2, w3, cv, dw[0], dw[1], hx, hy, lam, e2, e4, ftn);
             }
 
             // ---- n faces and the update of row m = k-3 ---------------------
@@ -527,13 +605,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     T hx = T(0.5) * nx2[0], hy = T(0.5) * ny2[0];
                     T dl[8];
                     for (int v = 0; v < 8; ++v) dl[v] = jst_shfl_up(dw[0][v], 1);
-                    for (int v = 0; v < 5; ++v) {
-                        T d1 = um[v] - ul1[v];
-                        T d3 = ur1[v] - T(3) * um[v] + T(3) * ul1[v] - ul2[v];
-                        T vis = T(0);
-                        if (v > 0) vis = (dl[v - 1] + dw[0][v - 1]) * hx + (dl[v + 3] + dw[0][v + 3]) * hy;
-                        fn[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
-                    }
+                    face_combine<T>(ul2, ul1, um, ur1, cv, dl, dw[0], hx, hy, lam, e2, e4, fn);
                 }
                 T fnr[5];
                 for (int v = 0; v < 5; ++v) fnr[v] = jst_shfl_down(fn[v], 1);
