@@ -427,15 +427,45 @@ def combine_batch_parts(parts: list, step_cap: int) -> dict:
     return out
 
 
-def serve_sweep(args):
+def serve_sweep(args, world: int = 1, rank: int = 0):
+    """Serving stream (config-5 draws) at each rate.  With several ranks the
+    request stream is dealt round-robin (request k to rank k mod N), which
+    splits the Poisson arrivals into N Poisson streams of rate R/N; each rank
+    serves its share on its own GPU and rank 0 prints the job figures."""
     from purinecfd_b200.serve import request_stream, serve
     out = []
     for rate in [float(x) for x in args.serve_rates.split(",")]:
-        reqs = request_stream(20261203, args.serve_requests, max_steps=args.batch_steps)
-        st, _ = serve(reqs, rate, seed=int(rate))
-        out.append(st.__dict__)
-        print(json.dumps({"serve": st.__dict__}), flush=True)
+        reqs = request_stream(20261203, args.serve_requests, max_steps=args.batch_steps)[rank::world]
+        barrier(world)
+        st, results = serve(reqs, rate / world, seed=int(rate) * world + rank) if reqs else (None, [])
+        part = {"rate": rate, "requests": len(reqs), "completed": len(results),
+                "converged": sum(1 for x in results if x[1].status == 0),
+                "nonphysical": sum(1 for x in results if x[1].status == 8),
+                "wall_s": st.wall_s if st else 0.0, "latencies": [x[2] for x in results],
+                "steps": [x[1].steps for x in results]}
+        parts = gather_objects(part, world)
+        if rank == 0:
+            job = combine_serve_parts(parts)
+            out.append(job)
+            print(json.dumps({"serve": job}), flush=True)
     return out
+
+
+def combine_serve_parts(parts: list) -> dict:
+    """Job-level serving figures from the per-rank parts: all requests count,
+    the job lasts as long as the slowest rank, latency percentiles over every
+    request."""
+    from purinecfd_b200.serve import percentile
+    wall = max(p["wall_s"] for p in parts)
+    lat = [x for p in parts for x in p["latencies"]]
+    steps = [x for p in parts for x in p["steps"]]
+    done = sum(p["completed"] for p in parts)
+    return {"rate": parts[0]["rate"], "ranks": len(parts), "requests": sum(p["requests"] for p in parts),
+            "completed": done, "converged": sum(p["converged"] for p in parts),
+            "nonphysical": sum(p["nonphysical"] for p in parts), "wall_s": wall,
+            "solves_per_s": done / wall if wall > 0 else None,
+            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99),
+            "mean_steps": sum(steps) / len(steps) if steps else None}
 
 
 def main():
@@ -463,7 +493,7 @@ def main():
                                                                    int(os.environ.get("RANK", "0")), 0)
     try:
         if args.serve:
-            serve_sweep(args)
+            serve_sweep(args, world, rank)
             return
         if args.impl == "reference":
             run_reference(args, world, rank)

@@ -90,3 +90,20 @@ def test_single_rank_needs_no_process_group():
     assert bench.max_over_ranks(3.5, 1) == 3.5
     bench.barrier(1)
     assert bench.replica_value(100, 2, 1.0, 1) == pytest.approx(100 * 5 * 2 / 1e-3 / 1e6)
+
+
+def test_serve_parts_combine_to_job_figures():
+    """Two ranks serving 3 + 2 requests: counts add, the slowest rank's wall
+    time is the job's, percentiles run over every request."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    parts = [{"rate": 50.0, "requests": 3, "completed": 3, "converged": 1, "nonphysical": 0, "wall_s": 2.0,
+              "latencies": [0.1, 0.2, 0.3], "steps": [100, 200, 300]},
+             {"rate": 50.0, "requests": 2, "completed": 2, "converged": 2, "nonphysical": 1, "wall_s": 2.5,
+              "latencies": [0.4, 0.5], "steps": [400, 500]}]
+    j = bench.combine_serve_parts(parts)
+    assert j["ranks"] == 2 and j["requests"] == 5 and j["completed"] == 5
+    assert j["converged"] == 3 and j["nonphysical"] == 1
+    assert j["wall_s"] == 2.5 and j["solves_per_s"] == pytest.approx(2.0)
+    assert j["p50_s"] == pytest.approx(0.3) and 0.45 < j["p99_s"] <= 0.5
+    assert j["mean_steps"] == pytest.approx(300.0)
