@@ -29,10 +29,6 @@
 
 #include "jst_common.cuh"
 
-#ifndef JST_PREFETCH_UN
-#define JST_PREFETCH_UN 0  // stage the tile's U_n in shared memory with the geometry
-#endif
-
 #ifndef JST_DYN_SMEM
 #define JST_DYN_SMEM(name) extern __shared__ __align__(16) unsigned char name[]
 #endif
@@ -98,7 +94,7 @@ struct TileRef {
 };
 
 // Shared-memory layout of one tile.  T-typed arrays first, then the FP64
-// block (geometry and the tile's U_n), then the reduction / far-field
+// block (the tile's geometry), then the reduction / far-field
 // scratch.  The primitive arrays (P, Q) are dead once gradients and sensors
 // exist, and the face fluxes reuse their space.
 template <class T, int TI, int TJ, int NT> struct Layout {
@@ -122,7 +118,7 @@ template <class T, int TI, int TJ, int NT> struct Layout {
     // FP64 geometry block: tau nx, ny; n nx, ny; 1/V on tile + ring; V and 1/d^2 on the tile
     static constexpr size_t goff = ((size_t)tsize * sizeof(T) + 15) / 16 * 16;
     static constexpr int gTx = 0, gTy = NGT, gNx = 2 * NGT, gNy = 2 * NGT + NGN, gIV = 2 * NGT + 2 * NGN,
-                         gV = gIV + NR, gD2 = gV + TT, gUn = gD2 + TT, gsize = gUn + (JST_PREFETCH_UN ? 5 * TT : 0);
+                         gV = gIV + NR, gD2 = gV + TT, gsize = gD2 + TT;
     static constexpr size_t red_off = goff + (size_t)gsize * sizeof(double);
     static constexpr size_t bytes = red_off + (size_t)(NT + 7 * LJ) * sizeof(double);
 };
@@ -446,14 +442,6 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
             gs[L::gD2 + e] = 0.0;
         }
     }
-#if JST_PREFETCH_UN
-    for (int e = tid; e < TT; e += NT) {  // U_n of the tile cells, for the update
-        int r = e / TJ, cc = e - r * TJ;
-        int gi = i0 + r, gj = j0 + cc;
-        if (gi < ni && gj < nj)
-            for (int k = 0; k < 5; ++k) async_copy<8>(gs + L::gUn + k * TT + e, I.un[k] + (long)gi * nj + gj);
-    }
-#endif
     constexpr int KA = (NL + NT - 1) / NT;
     TS rawr[ASYNC_U ? 1 : KA][5];
 #pragma unroll
@@ -714,11 +702,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
         if (gi >= ni || gj >= nj) continue;
         long id = (long)gi * nj + gj;
         double uo[5];
-#if JST_PREFETCH_UN
-        for (int k = 0; k < 5; ++k) uo[k] = gs[L::gUn + k * TT + w];
-#else
         for (int k = 0; k < 5; ++k) uo[k] = I.un[k][id];
-#endif
         T R[5];
         const int fd = ti * (TJ + 1) + tj;
         for (int k = 0; k < 5; ++k)
