@@ -1597,6 +1597,32 @@ struct jst_batch {
     std::unique_ptr<jst::BatchBase> impl;
 };
 
+// Test hook (not in the public header): the marching kernels' FP64 quotient
+// and square root (jst::dv / jst::sq with Q = true) beside the correctly
+// rounded ones, for n operand pairs: out[4k..4k+3] = quick a/b, a/b, quick
+// sqrt(b), sqrt(b).
+__global__ void k_quick_arith(const double* a, const double* b, double* out, long n) {
+    long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double x = a[k], y = b[k];
+    out[4 * k + 0] = jst::dv<double, true>(x, y);
+    out[4 * k + 1] = __ddiv_rn(x, y);
+    out[4 * k + 2] = jst::sq<double, true>(y);
+    out[4 * k + 3] = __dsqrt_rn(y);
+}
+
+extern "C" jst_status jst_debug_quick_arith(const double* a, const double* b, double* out, size_t n) {
+    if (!a || !b || !out || n == 0) return JST_ERR_ARG;
+    double* d = nullptr;
+    if (cudaMalloc(&d, 6 * n * sizeof(double)) != cudaSuccess) return JST_ERR_OOM;
+    cudaMemcpy(d, a, n * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(d + n, b, n * sizeof(double), cudaMemcpyHostToDevice);
+    JST_LAUNCH(k_quick_arith, (unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)0, d, d + n, d + 2 * n, (long)n);
+    cudaError_t e = cudaMemcpy(out, d + 2 * n, 4 * n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? JST_OK : JST_ERR_CUDA;
+}
+
 extern "C" {
 
 void jst_batch_default_opts(jst_batch_opts* o) {

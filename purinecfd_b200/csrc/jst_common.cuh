@@ -58,6 +58,43 @@ template <class T> JST_HD T powi6(T x) {
     return x2 * x4;
 }
 
+// Quotient and square root for the fused kernels (Q = true); the strict
+// passes path keeps the library's correctly rounded / and sqrt (Q = false).
+// In double on the device they avoid the library routines' special-case
+// branch, which splits the instruction scheduler's basic blocks in the middle
+// of every cell's arithmetic:
+//  * a / b: the hardware reciprocal approximation of b refined by one
+//    third-order Newton-Raphson step r <- r (1 + e + e^2), e = 1 - b r (the
+//    relative error is cubed), then one residual correction of the quotient
+//    q <- q + r (a - b q) (Markstein, IA-64 and Elementary Functions, 2000);
+//  * sqrt(x): the hardware reciprocal square root approximation y refined by
+//    one Newton-Raphson step y <- y (3/2 - x y^2 / 2), then the correction
+//    s <- s + (y / 2) (x - s^2) of s = x y (same reference).
+// Both stay within one unit in the last place of the correctly rounded
+// result for normal finite operands (b != 0, x > 0), which is all these
+// kernels divide by or take roots of; a NaN operand gives NaN.  In float the
+// translation unit's division and root are used as they are.
+template <class T, bool Q = false> JST_HD T dv(T a, T b) { return a / b; }
+template <class T, bool Q = false> JST_HD T sq(T x) { return sqrt(x); }
+#ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ double dv<double, true>(double a, double b) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+    const double e = fma(-b, r, 1.0);
+    r = fma(r, fma(e, e, e), r);
+    const double q = a * r;
+    return fma(r, fma(-b, q, a), q);
+}
+template <> __device__ __forceinline__ double sq<double, true>(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * y;
+    y = fma(h, fma(-x * y, y, 1.0), y);
+    const double s = x * y;
+    return fma(0.5 * y, fma(-s, s, x), s);
+}
+#endif
+
 template <class T> JST_HD T tmax(T a, T b) { return fmax(a, b); }
 template <class T> JST_HD T tmin(T a, T b) { return fmin(a, b); }
 template <> JST_HD float tmax<float>(float a, float b) { return fmaxf(a, b); }
@@ -69,16 +106,16 @@ template <class T> struct Prim {
 };
 
 // Solver::unpack (solver.rs:158-181) for one cell, without the checks.
-template <class T> JST_HD Prim<T> unpack_cell(T u0, T u1, T u2, T u3, T u4, T gm1, T r_gas) {
+template <class T, bool Q = false> JST_HD Prim<T> unpack_cell(T u0, T u1, T u2, T u3, T u4, T gm1, T r_gas) {
     Prim<T> q;
     T rho = u0;
-    T inv = T(1) / rho;
+    T inv = dv<T, Q>(T(1), rho);
     q.rho = rho;
     q.vx = u1 * inv;
     q.vy = u2 * inv;
     q.e = u3 * inv;
     q.p = gm1 * (u3 - rho * (q.vx * q.vx + q.vy * q.vy) * T(0.5));
-    q.t = q.p / (r_gas * rho);
+    q.t = dv<T, Q>(q.p, r_gas * rho);
     q.nut = u4 * inv;
     return q;
 }
@@ -93,9 +130,9 @@ template <class T> JST_HD void pack_cell(const Prim<T>& q, T* u) {
 }
 
 // Config::mu, Sutherland (config.rs:287-291).
-template <class T> JST_HD T mu_of(T t, T inv_t_ref, T suth_num, T t_suth) {
+template <class T, bool Q = false> JST_HD T mu_of(T t, T inv_t_ref, T suth_num, T t_suth) {
     T r = t * inv_t_ref;
-    return r * sqrt(r) * suth_num / (t + t_suth);
+    return dv<T, Q>(r * sq<T, Q>(r) * suth_num, t + t_suth);
 }
 
 // convection::euler_flux (convection.rs:25-40): F.n of the face state fu.
@@ -104,9 +141,10 @@ template <class T> JST_HD T mu_of(T t, T inv_t_ref, T suth_num, T t_suth) {
 // in FP32 the large constant part of p no longer cancels between the two
 // faces of a thin wall cell.  The FP64 paths pass p_ref = 0, i.e. the
 // reference's formula.
-template <class T> JST_HD void euler_flux(const T fu[5], T nx, T ny, T gm1, T out[5], T p_ref = T(0)) {
+template <class T, bool Q = false>
+JST_HD void euler_flux(const T fu[5], T nx, T ny, T gm1, T out[5], T p_ref = T(0)) {
     T rho = fu[0];
-    T inv_rho = T(1) / rho;
+    T inv_rho = dv<T, Q>(T(1), rho);
     T u = fu[1] * inv_rho;
     T v = fu[2] * inv_rho;
     T rho_e = fu[3];
@@ -155,15 +193,15 @@ template <class T> struct Diff {
     T dx1, dx2, dx3, dx4, dy1, dy2, dy3, dy4;
 };
 
-template <class T>
+template <class T, bool Q = false>
 JST_HD Diff<T> diffusion_tensor(T t, T rho_nu, T vx, T vy, T dudx, T dudy, T dvdx, T dvdy, T dtdx, T dtdy, T dnx,
                                 T dny, T inv_t_ref, T suth_num, T t_suth, T cv1_cubed, T inv_pr, T inv_prt, T cp,
                                 T sigma) {
     Diff<T> d;
-    T mu = mu_of<T>(t, inv_t_ref, suth_num, t_suth);
-    T chi = rho_nu / mu;
+    T mu = mu_of<T, Q>(t, inv_t_ref, suth_num, t_suth);
+    T chi = dv<T, Q>(rho_nu, mu);
     T c3 = chi * chi * chi;  // viscous.rs:27-30
-    T f1 = c3 / (c3 + cv1_cubed);
+    T f1 = dv<T, Q>(c3, c3 + cv1_cubed);
     T mu_t = rho_nu * f1;
     T mu_eff = mu + mu_t;
     T lam_eff = mu * inv_pr + mu_t * inv_prt;
@@ -188,14 +226,14 @@ JST_HD Diff<T> diffusion_tensor(T t, T rho_nu, T vx, T vy, T dudx, T dudy, T dvd
 }
 
 // dissipation::pressure_sensor (dissipation.rs:29-31).
-template <class T> JST_HD T pressure_sensor(T pm, T p0, T pp) {
-    return fabs((pm - T(2) * p0 + pp) / (pm + T(2) * p0 + pp));
+template <class T, bool Q = false> JST_HD T pressure_sensor(T pm, T p0, T pp) {
+    return fabs(dv<T, Q>(pm - T(2) * p0 + pp, pm + T(2) * p0 + pp));
 }
 
 // source::fw (source.rs:30-33).
-template <class T> JST_HD T fw_of(T r, T cw2, T cw3_6, T one_plus_cw3_6) {
+template <class T, bool Q = false> JST_HD T fw_of(T r, T cw2, T cw3_6, T one_plus_cw3_6) {
     T g = r + cw2 * (powi6<T>(r) - r);
-    return g * cbrt(sqrt(one_plus_cw3_6 / (powi6<T>(g) + cw3_6)));
+    return g * cbrt(sq<T, Q>(dv<T, Q>(one_plus_cw3_6, powi6<T>(g) + cw3_6)));
 }
 
 // fw for the FP32 path.  Near the wall a slightly negative nu-tilde over
@@ -231,21 +269,21 @@ JST_HD float fw_of_f32(float r, double cw2, double cw3_6, double one_plus_cw3_6,
 }
 
 // source::compute for one cell (source.rs:55-85), before the factor V.
-template <class T>
+template <class T, bool Q = false>
 JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny, const PhysConst& c) {
-    T nu_tilde = rho_nu / rho;
+    T nu_tilde = dv<T, Q>(rho_nu, rho);
     T inv_kd2 = inv_dist2 * T(c.inv_kappa2);
     T ft2;
     if constexpr (sizeof(T) == sizeof(float)) ft2 = T(c.Ct3) * exp_f32(-T(c.Ct4) * chi * chi);
     else ft2 = T(c.Ct3) * exp(-T(c.Ct4) * chi * chi);
-    T fv2 = T(1) - chi / (T(1) + chi * f1);
+    T fv2 = T(1) - dv<T, Q>(chi, T(1) + chi * f1);
     T sv = T(c.fv3) * fabs(dvdx - dudy);
     T s_tilde = tmax<T>(sv + nu_tilde * inv_kd2 * fv2, T(1e-10));
     T prod = T(c.Cb1) * (T(1) - ft2) * s_tilde * rho_nu;
-    T r = tmin<T>(nu_tilde / s_tilde * inv_kd2, T(c.rmax));
+    T r = tmin<T>(dv<T, Q>(nu_tilde, s_tilde) * inv_kd2, T(c.rmax));
     T fw;
     if constexpr (sizeof(T) == sizeof(float)) fw = fw_of_f32(r, c.Cw2, c.cw3_6, c.one_plus_cw3_6, c.fw_lim);
-    else fw = fw_of<T>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6));
+    else fw = fw_of<T, Q>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6));
     T destr = (T(c.cw1) * fw - T(c.cb1_k2) * ft2) * rho * (nu_tilde * nu_tilde * inv_dist2);
     T diff = T(c.cb2_sigma) * rho * (dnx * dnx + dny * dny);
     return prod - destr + diff;
@@ -323,10 +361,10 @@ JST_HD FarState riemann_face(double fnx, double fny, double ui, double vi, doubl
 
 // timestep::compute for one cell (timestep.rs:30-42): a,b / cc,dd are the
 // averaged tau / n normals.
-template <class T> JST_HD T local_dt(T u, T v, T cs, T a, T b, T cc, T dd, T cfl_vol) {
+template <class T, bool Q = false> JST_HD T local_dt(T u, T v, T cs, T a, T b, T cc, T dd, T cfl_vol) {
     T conv = fabs(u * a + v * b) + fabs(u * cc + v * dd);
-    T acou = cs * (sqrt(a * a + b * b) + sqrt(cc * cc + dd * dd));
-    return cfl_vol / (conv + acou);
+    T acou = cs * (sq<T, Q>(a * a + b * b) + sq<T, Q>(cc * cc + dd * dd));
+    return dv<T, Q>(cfl_vol, conv + acou);
 }
 
 }  // namespace jst

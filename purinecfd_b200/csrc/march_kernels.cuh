@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     p.e = (T)c.f_e;
                     p.nut = (T)c.f_nut;
                 } else {
-                    p = unpack_cell<T>(uk[0], uk[1], uk[2], uk[3], uk[4], gm1, rgas);
+                    p = unpack_cell<T, true>(uk[0], uk[1], uk[2], uk[3], uk[4], gm1, rgas);
                 }
                 if (seam) pack_cell<T>(p, uk);  // periodic ghost column (boundary.rs:54-72)
                 if (wall) {
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     q.vx = -p.vx;
                     q.vy = -p.vy;
                     q.nut = -p.nut;
-                    q.e = fresh ? (T)c.f_e : uk[3] * (T(1) / q.rho);
+                    q.e = fresh ? (T)c.f_e : uk[3] * dv<T, true>(T(1), q.rho);
                     pack_cell<T>(q, uk);
                     p = q;
                 }
@@ -461,9 +461,9 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 for (int v = 0; v < 4; ++v) qk[v] = qw[1][v];
             }
             // j-sensor of row k (dissipation.rs:73-90)
-            const T sjk = pressure_sensor<T>(jst_shfl_up(pk, 1), pk, jst_shfl_down(pk, 1));
+            const T sjk = pressure_sensor<T, true>(jst_shfl_up(pk, 1), pk, jst_shfl_down(pk, 1));
             // i-sensor of row k-1
-            const T sik = pressure_sensor<T>(pw[0], pw[1], pk);
+            const T sik = pressure_sensor<T, true>(pw[0], pw[1], pk);
 
             // ---- geometry record of row k (tau normals of face row k; n
             // normals, 1/V, 1/d^2, V of cell row k-1) -------------------------
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                             green_gauss_delta<T>(cq, qk[q], qw[0][q], lf, rg, txk, tyk, tx[2], ty[2], nxr, nyr, rtx,
                                                  rty, iv, &g[2 * q], &g[2 * q + 1]);
                     }
-                    Diff<T> d = diffusion_tensor<T>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], g[0], g[1], g[2], g[3], g[4],
+                    Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], g[0], g[1], g[2], g[3], g[4],
                                                     g[5], g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num, (T)c.t_suth,
                                                     (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp, (T)c.sigma);
                     dn[0] = d.dx1;
@@ -514,13 +514,13 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     dn[6] = d.dy3;
                     dn[7] = d.dy4;
                     if (S || (r >= i0 && r < i1)) {
-                        T s5 = sa_source<T>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
+                        T s5 = sa_source<T, true>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
                         snew = s5 * gk[MG_VOL];
                     }
                     if (!S && r == 0) {
                         // the wall ghost ring (row -1, one row up in the window) takes cell
                         // 0's gradient with grad T = 0 (gradient.rs:93-95)
-                        Diff<T> w = diffusion_tensor<T>(qw[0][2], UA(2, 4), qw[0][0], qw[0][1], g[0], g[1], g[2], g[3],
+                        Diff<T> w = diffusion_tensor<T, true>(qw[0][2], UA(2, 4), qw[0][0], qw[0][1], g[0], g[1], g[2], g[3],
                                                         T(0), T(0), g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num,
                                                         (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt,
                                                         (T)c.cp, (T)c.sigma);
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         dw[1][7] = w.dy4;
                     }
                 } else if (r >= ni) {  // far ghost ring: zero gradient (gradient.rs:96)
-                    Diff<T> d = diffusion_tensor<T>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], T(0), T(0), T(0), T(0),
+                    Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], T(0), T(0), T(0), T(0),
                                                     T(0), T(0), T(0), T(0), (T)c.inv_t_ref, (T)c.suth_num,
                                                     (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp,
                                                     (T)c.sigma);
@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     fu[v] = T(0.5) * (w1[v] + w2[v]);
                 }
                 const T fnx = tx[1], fny = ty[1];
-                euler_flux<T>(fu, fnx, fny, gm1, cv, p_ref);
+                euler_flux<T, true>(fu, fnx, fny, gm1, cv, p_ref);
                 T hx = T(0.5) * fnx, hy = T(0.5) * fny;
                 face_combine<T>(w0, w1, w2, w3, cv, dw[0], dw[1], hx, hy, lam, e2, e4, ftn);
             }
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         ur1[v] = jst_shfl_down(um[v], 1);
                         fu[v] = T(0.5) * (ul1[v] + um[v]);
                     }
-                    euler_flux<T>(fu, nx2[0], ny2[0], gm1, cv, p_ref);
+                    euler_flux<T, true>(fu, nx2[0], ny2[0], gm1, cv, p_ref);
                     T hx = T(0.5) * nx2[0], hy = T(0.5) * ny2[0];
                     T dl[8];
                     for (int v = 0; v < 8; ++v) dl[v] = jst_shfl_up(dw[0][v], 1);
@@ -644,14 +644,14 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         double rho = un[0];
                         bad = isnan(rho) || rho <= 1e-15;
                         if (!bad) {
-                            q = unpack_cell<double>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
+                            q = unpack_cell<double, true>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
                             bad = isnan(q.p) || q.p <= 1e-15;
                         }
                     } else {
                         T rho = (T)un[0];
                         bad = isnan(rho) || rho <= T(1e-15);
                         if (!bad) {
-                            Prim<T> qt = unpack_cell<T>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], gm1, rgas);
+                            Prim<T> qt = unpack_cell<T, true>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], gm1, rgas);
                             bad = isnan(qt.p) || qt.p <= T(1e-15);
                             q.vx = qt.vx;
                             q.vy = qt.vy;
@@ -670,8 +670,8 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         T dd = T(0.5) * (ny2[0] + nyr3);
                         T vol = PIPE ? B->volm[lane] : ld(I.mg + MG_N * (id + nj) + MG_VOL);
                         T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
-                        T dl = local_dt<T>(qvx, qvy, sqrt((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
-                        ratio_next[id] = vol / dl;
+                        T dl = local_dt<T, true>(qvx, qvy, sq<T, true>((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
+                        ratio_next[id] = dv<T, true>(vol, dl);
                         if (dt_local) I.ldt[id] = (double)dl;
                         mloc = fmin(mloc, (double)dl);
                     }
@@ -723,9 +723,20 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         };
         const int ks0 = i0 + 3, ks1 = i1 - 2;  // steady rows
         int k = i0 - 3;
-        for (; k < ks0 && k <= i1 + 2; ++k) row(std::false_type{}, k);
-        for (; k <= ks1; ++k) row(std::true_type{}, k);
-        for (; k <= i1 + 2; ++k) row(std::false_type{}, k);
+        if constexpr (sizeof(T) == sizeof(double)) {
+            // The FP64 non-steady body, called from two sites, is compiled
+            // out of line (its captured windows then pass through the
+            // stack); a single call site keeps it inline.
+            for (int ph = 0; ph < 2; ++ph) {
+                for (; k <= (ph == 0 ? ks0 - 1 : i1 + 2) && k <= i1 + 2; ++k) row(std::false_type{}, k);
+                if (ph == 0)
+                    for (; k <= ks1; ++k) row(std::true_type{}, k);
+            }
+        } else {
+            for (; k < ks0 && k <= i1 + 2; ++k) row(std::false_type{}, k);
+            for (; k <= ks1; ++k) row(std::true_type{}, k);
+            for (; k <= i1 + 2; ++k) row(std::false_type{}, k);
+        }
 
         if (LAST) {
             double mn = warp_min(mloc);

@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
         L.jst_kernel_config.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.jst_debug_set_uniform.argtypes = [vp, d, d, d, d, d]
         L.jst_debug_kernel.argtypes = [vp, C.c_char_p]
+        L.jst_debug_quick_arith.argtypes = [pd, pd, pd, sz]
         _lib = L
     return _lib
 
