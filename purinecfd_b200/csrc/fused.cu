@@ -1597,28 +1597,34 @@ struct jst_batch {
     std::unique_ptr<jst::BatchBase> impl;
 };
 
-// Test hook (not in the public header): the marching kernels' FP64 quotient
-// and square root (jst::dv / jst::sq with Q = true) beside the correctly
-// rounded ones, for n operand pairs: out[4k..4k+3] = quick a/b, a/b, quick
-// sqrt(b), sqrt(b).
+// Test hook (not in the public header): the marching kernels' FP64
+// quotient, square root, exponential and inverse sixth root (jst::dv, sq, ex
+// with Q = true, and jst::rroot6) beside the library's, for n operand pairs:
+// out[8k..8k+7] = quick a/b, a/b, quick sqrt(b), sqrt(b), quick exp(a),
+// exp(a), b^(-1/6), 1 / cbrt(sqrt(b)).
 __global__ void k_quick_arith(const double* a, const double* b, double* out, long n) {
     long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const double x = a[k], y = b[k];
-    out[4 * k + 0] = jst::dv<double, true>(x, y);
-    out[4 * k + 1] = __ddiv_rn(x, y);
-    out[4 * k + 2] = jst::sq<double, true>(y);
-    out[4 * k + 3] = __dsqrt_rn(y);
+    double* o = out + 8 * k;
+    o[0] = jst::dv<double, true>(x, y);
+    o[1] = __ddiv_rn(x, y);
+    o[2] = jst::sq<double, true>(y);
+    o[3] = __dsqrt_rn(y);
+    o[4] = jst::ex<double, true>(x);
+    o[5] = exp(x);
+    o[6] = jst::rroot6(y);
+    o[7] = __ddiv_rn(1.0, cbrt(__dsqrt_rn(y)));
 }
 
 extern "C" jst_status jst_debug_quick_arith(const double* a, const double* b, double* out, size_t n) {
     if (!a || !b || !out || n == 0) return JST_ERR_ARG;
     double* d = nullptr;
-    if (cudaMalloc(&d, 6 * n * sizeof(double)) != cudaSuccess) return JST_ERR_OOM;
+    if (cudaMalloc(&d, 10 * n * sizeof(double)) != cudaSuccess) return JST_ERR_OOM;
     cudaMemcpy(d, a, n * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(d + n, b, n * sizeof(double), cudaMemcpyHostToDevice);
     JST_LAUNCH(k_quick_arith, (unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)0, d, d + n, d + 2 * n, (long)n);
-    cudaError_t e = cudaMemcpy(out, d + 2 * n, 4 * n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(out, d + 2 * n, 8 * n * sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(d);
     return e == cudaSuccess ? JST_OK : JST_ERR_CUDA;
 }

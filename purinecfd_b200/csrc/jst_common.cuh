@@ -95,6 +95,64 @@ template <> __device__ __forceinline__ double sq<double, true>(double x) {
 }
 #endif
 
+// exp for the fused kernels (Q = true), in double without the library
+// routine's range branch: Cody-Waite reduction x = n ln2 + r, |r| <= ln2/2,
+// with ln 2 split into a 42-bit head (n ln2_hi is exact for |n| < 2^11) and
+// its tail (Cody and Waite, Software Manual for the Elementary Functions,
+// 1980); the Taylor polynomial of e^r to degree 13 (truncation error below
+// 2^-57) in Horner form; the scaling by 2^n as two exact powers of two, so
+// that a result in the subnormal range is rounded once.  Arguments are
+// clamped to [-746, 710] (e^-746 rounds to 0, e^710 overflows); NaN gives NaN.
+template <class T, bool Q = false> JST_HD T ex(T x) { return exp(x); }
+#ifdef __CUDACC__
+// 2^n for -1022 <= n <= 1023, from the exponent field.
+__device__ __forceinline__ double pow2i(int n) { return __hiloint2double((n + 1023) << 20, 0); }
+#endif
+#ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ double ex<double, true>(double x) {
+    x = x < -746.0 ? -746.0 : (x > 710.0 ? 710.0 : x);
+    const double n = rint(x * 1.4426950408889634);  // log2(e)
+    const double r = fma(-n, 0x1.ef35793c7673p-45, fma(-n, 0x1.62e42fefa38p-1, x));
+    double p = 1.0 / 6227020800.0;  // 1/13!
+    p = fma(p, r, 1.0 / 479001600.0);
+    p = fma(p, r, 1.0 / 39916800.0);
+    p = fma(p, r, 1.0 / 3628800.0);
+    p = fma(p, r, 1.0 / 362880.0);
+    p = fma(p, r, 1.0 / 40320.0);
+    p = fma(p, r, 1.0 / 5040.0);
+    p = fma(p, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    const int k = (int)n, k1 = k / 2;
+    return p * pow2i(k1) * pow2i(k - k1);
+}
+#endif
+
+#ifdef __CUDACC__
+// d^(-1/6) for d > 0 in double without library calls or branches: d is
+// scaled by the exact power of two 2^(-6m) into [1, 64); an FP32 estimate of
+// the scaled root from the hardware base-2 logarithm and exponential is
+// refined by two Newton-Raphson steps for t^-6 = d, t <- t + t (1 - d t^6) / 6
+// (each squares the relative error), and multiplied by 2^-m.  d = +inf gives
+// 0 (the limit), NaN gives NaN.
+__device__ __forceinline__ double rroot6(double d) {
+    const int e = ((__double2hiint(d) >> 20) & 0x7ff) - 1023;
+    const int m = (e + 1200) / 6 - 200;  // floor(e / 6) for e >= -1200
+    const double ds = d * pow2i(-3 * m) * pow2i(-3 * m);
+    double t = (double)exp2f(__log2f((float)ds) * (-1.0f / 6.0f));
+    for (int it = 0; it < 2; ++it) {
+        const double t2 = t * t;
+        t = fma(t * (1.0 / 6.0), fma(-ds, t2 * t2 * t2, 1.0), t);
+    }
+    t *= pow2i(-m);
+    return isinf(d) ? 0.0 : t;
+}
+#endif
+
 template <class T> JST_HD T tmax(T a, T b) { return fmax(a, b); }
 template <class T> JST_HD T tmin(T a, T b) { return fmin(a, b); }
 template <> JST_HD float tmax<float>(float a, float b) { return fmaxf(a, b); }
@@ -231,8 +289,15 @@ template <class T, bool Q = false> JST_HD T pressure_sensor(T pm, T p0, T pp) {
 }
 
 // source::fw (source.rs:30-33).
-template <class T, bool Q = false> JST_HD T fw_of(T r, T cw2, T cw3_6, T one_plus_cw3_6) {
+// With Q in double on the device, the root of the quotient is taken as
+// fw_lim * (g^6 + Cw3^6)^(-1/6), fw_lim = (1 + Cw3^6)^(1/6) (the same value
+// within a few units in the last place, one division fewer).
+template <class T, bool Q = false> JST_HD T fw_of(T r, T cw2, T cw3_6, T one_plus_cw3_6, T fw_lim) {
     T g = r + cw2 * (powi6<T>(r) - r);
+#ifdef __CUDA_ARCH__
+    if constexpr (Q && sizeof(T) == sizeof(double)) return g * fw_lim * rroot6(powi6<T>(g) + cw3_6);
+#endif
+    (void)fw_lim;
     return g * cbrt(sq<T, Q>(dv<T, Q>(one_plus_cw3_6, powi6<T>(g) + cw3_6)));
 }
 
@@ -275,7 +340,7 @@ JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T 
     T inv_kd2 = inv_dist2 * T(c.inv_kappa2);
     T ft2;
     if constexpr (sizeof(T) == sizeof(float)) ft2 = T(c.Ct3) * exp_f32(-T(c.Ct4) * chi * chi);
-    else ft2 = T(c.Ct3) * exp(-T(c.Ct4) * chi * chi);
+    else ft2 = T(c.Ct3) * ex<T, Q>(-T(c.Ct4) * chi * chi);
     T fv2 = T(1) - dv<T, Q>(chi, T(1) + chi * f1);
     T sv = T(c.fv3) * fabs(dvdx - dudy);
     T s_tilde = tmax<T>(sv + nu_tilde * inv_kd2 * fv2, T(1e-10));
@@ -283,7 +348,7 @@ JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T 
     T r = tmin<T>(dv<T, Q>(nu_tilde, s_tilde) * inv_kd2, T(c.rmax));
     T fw;
     if constexpr (sizeof(T) == sizeof(float)) fw = fw_of_f32(r, c.Cw2, c.cw3_6, c.one_plus_cw3_6, c.fw_lim);
-    else fw = fw_of<T, Q>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6));
+    else fw = fw_of<T, Q>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6), T(c.fw_lim));
     T destr = (T(c.cw1) * fw - T(c.cb1_k2) * ft2) * rho * (nu_tilde * nu_tilde * inv_dist2);
     T diff = T(c.cb2_sigma) * rho * (dnx * dnx + dny * dny);
     return prod - destr + diff;

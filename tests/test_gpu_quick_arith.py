@@ -1,8 +1,10 @@
-"""The marching kernels' FP64 quotient and square root (hardware reciprocal /
-reciprocal-root approximations refined by Newton-Raphson steps and a residual
-correction) against CUDA's correctly rounded division and root: at most one
-unit in the last place apart over operands spanning sixty decades, and NaN
-in, NaN out."""
+"""The marching kernels' FP64 quotient, square root, exponential and inverse
+sixth root (hardware approximations refined by Newton-Raphson steps; Cody-Waite
+reduction and a Taylor polynomial) against CUDA's: the quotient and root at
+most one unit in the last place from the correctly rounded ones over operands
+spanning sixty decades, the exponential within two units of CUDA's exp, the
+inverse sixth root within four units of 1 / cbrt(sqrt(d)), and NaN in, NaN
+out."""
 
 from __future__ import annotations
 
@@ -18,11 +20,11 @@ def _run(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     from purinecfd_b200.solver import OK, lib
     a = np.ascontiguousarray(a, dtype=np.float64)
     b = np.ascontiguousarray(b, dtype=np.float64)
-    out = np.empty(4 * a.size)
+    out = np.empty(8 * a.size)
     pd = C.POINTER(C.c_double)
     rc = lib().jst_debug_quick_arith(a.ctypes.data_as(pd), b.ctypes.data_as(pd), out.ctypes.data_as(pd), a.size)
     assert rc == OK
-    return out.reshape(-1, 4)
+    return out.reshape(-1, 8)
 
 
 def _ulps(x: np.ndarray, y: np.ndarray) -> np.ndarray:
@@ -66,3 +68,27 @@ def test_nan_propagates():
     r = _run(a, b)
     assert np.all(np.isnan(r[:, 0]))
     assert np.isnan(r[1, 2]) and np.isnan(r[2, 2])
+    assert np.isnan(r[0, 4]) and np.isnan(r[1, 6]) and np.isnan(r[2, 6])
+
+
+def test_exp_within_two_ulps():
+    rng = np.random.default_rng(11)
+    n = 1 << 20
+    a = np.concatenate([rng.uniform(-745.0, 709.0, n // 2), rng.uniform(-40.0, 40.0, n // 2)])
+    a[:6] = [0.0, 1.0, -1.0, -2e8, -0.5 * np.log(2.0), 700.0]
+    r = _run(a, np.ones_like(a))
+    assert r[0, 4] == 1.0
+    assert r[3, 4] == 0.0 and r[3, 5] == 0.0
+    assert _ulps(r[:, 4], r[:, 5]).max() <= 2
+
+
+def test_inverse_sixth_root_within_four_ulps():
+    rng = np.random.default_rng(13)
+    n = 1 << 20
+    b = 10.0 ** rng.uniform(-300.0, 300.0, n)
+    b[:4] = [64.0, 1.0, 2.0 ** 60, 4096.0]
+    r = _run(np.ones_like(b), b)
+    assert r[0, 6] == 0.5 and r[1, 6] == 1.0 and r[2, 6] == 2.0 ** -10 and r[3, 6] == 0.25
+    assert _ulps(r[:, 6], r[:, 7]).max() <= 4
+    special = _run(np.ones(2), np.array([np.inf, np.nan]))
+    assert special[0, 6] == 0.0 and np.isnan(special[1, 6])
