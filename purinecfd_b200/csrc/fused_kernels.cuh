@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
                     p.e = (T)c.f_e;
                     p.nut = (T)c.f_nut;
                 } else {
-                    p = unpack_cell<T>(u[0], u[1], u[2], u[3], u[4], (T)c.gm1, (T)c.r_gas);
+                    p = unpack_cell<T, true>(u[0], u[1], u[2], u[3], u[4], (T)c.gm1, (T)c.r_gas);
                 }
                 bool seam = gjr < 0 || gjr >= nj;
                 if (seam) pack_cell<T>(p, u);
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
                 q.vx = -sQ[os];
                 q.vy = -sQ[NL + os];
                 q.nut = -sQ[3 * NL + os];
-                q.e = fresh ? (T)c.f_e : sU[3 * NL + os] * (T(1) / q.rho);
+                q.e = fresh ? (T)c.f_e : sU[3 * NL + os] * dv<T, true>(T(1), q.rho);
             } else {
                 const double* fb = farbuf + 7 * lj;
                 q.rho = (T)fb[0];
@@ -568,12 +568,12 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
     for (int w = tid; w < L::NSI; w += NT) {  // i-direction, rows i0-2 .. i0+TI+1
         int r = w / TJ, tj = w - r * TJ;
         int o = (r + 1) * LJ + tj + 3;
-        sSi[w] = pressure_sensor<T>(sP[o - LJ], sP[o], sP[o + LJ]);
+        sSi[w] = pressure_sensor<T, true>(sP[o - LJ], sP[o], sP[o + LJ]);
     }
     for (int w = tid; w < L::NSJ; w += NT) {  // j-direction, columns j0-2 .. j0+TJ+1
         int ti = w / (TJ + 4), cc = w - ti * (TJ + 4);
         int o = (ti + 3) * LJ + cc + 1;
-        sSj[w] = pressure_sensor<T>(sP[o - 1], sP[o], sP[o + 1]);
+        sSj[w] = pressure_sensor<T, true>(sP[o - 1], sP[o], sP[o + 1]);
     }
 
     // ---- B2: gradients, diffusion tensors (tile + ring), SA source (tile) -
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
             }
         }
         int o = li * LJ + lj;
-        Diff<T> d = diffusion_tensor<T>(sQ[2 * NL + o], sU[4 * NL + o], sQ[0 * NL + o], sQ[1 * NL + o], g[0], g[1],
+        Diff<T> d = diffusion_tensor<T, true>(sQ[2 * NL + o], sU[4 * NL + o], sQ[0 * NL + o], sQ[1 * NL + o], g[0], g[1],
                                         g[2], g[3], g[4], g[5], g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num,
                                         (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp,
                                         (T)c.sigma);
@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
         sD[7 * NR + w] = d.dy4;
         if (ri >= 1 && ri <= TI && rj >= 1 && rj <= TJ) {
             int tcell = (ri - 1) * TJ + (rj - 1);
-            T s5 = sa_source<T>(sU[o], sU[4 * NL + o], (T)gs[L::gD2 + tcell], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
+            T s5 = sa_source<T, true>(sU[o], sU[4 * NL + o], (T)gs[L::gD2 + tcell], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
             sS[tcell] = s5 * (T)gs[L::gV + tcell];
         }
     }
@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
         lam = half_cfl * (sRat[db] + sRat[da]);
         T fu[5], cv[5];
         for (int k = 0; k < 5; ++k) fu[k] = T(0.5) * (sU[k * NL + lo - step] + sU[k * NL + lo]);
-        euler_flux<T>(fu, nx, ny, gm1, cv, p_ref);
+        euler_flux<T, true>(fu, nx, ny, gm1, cv, p_ref);
         T hx = T(0.5) * nx, hy = T(0.5) * ny;
         T* out = tau ? sFt + w : sFn + (w - L::NFT);
         const int ostride = tau ? L::NFT : L::NFN;
@@ -725,14 +725,14 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
             double rho = un[0];
             bad = isnan(rho) || rho <= 1e-15;
             if (!bad) {
-                q = unpack_cell<double>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
+                q = unpack_cell<double, true>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
                 bad = isnan(q.p) || q.p <= 1e-15;
             }
         } else {
             T rho = (T)un[0];
             bad = isnan(rho) || rho <= T(1e-15);
             if (!bad) {
-                Prim<T> qt = unpack_cell<T>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], (T)c.gm1, (T)c.r_gas);
+                Prim<T> qt = unpack_cell<T, true>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], (T)c.gm1, (T)c.r_gas);
                 bad = isnan(qt.p) || qt.p <= T(1e-15);
                 q.vx = qt.vx;
                 q.vy = qt.vy;
@@ -755,8 +755,8 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
             T dd = T(0.5) * ((T)gs[L::gNy + nlf] + (T)gs[L::gNy + nrt]);
             T vol = (T)gs[L::gV + w];
             T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
-            T dl = local_dt<T>(qvx, qvy, sqrt((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
-            ratio_next[id] = vol / dl;
+            T dl = local_dt<T, true>(qvx, qvy, sq<T, true>((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
+            ratio_next[id] = dv<T, true>(vol, dl);
             if (I.local_dt) I.ldt[id] = (double)dl;
             mloc = fmin(mloc, (double)dl);
         }
