@@ -328,9 +328,11 @@ JST_HD float exp_f32(float x) {
 JST_HD float fw_of_f32(float r, double cw2, double cw3_6, double one_plus_cw3_6, double fw_lim) {
     double rd = (double)r;
     double g = rd + cw2 * (powi6<double>(rd) - rd);
-    if (g > 1e5) return (float)fw_lim;
-    float gf = (float)g;
-    return gf * root6_f32((float)one_plus_cw3_6 / (powi6<float>(gf) + (float)cw3_6));
+    // both sides evaluated and selected (no branch); g is clamped first so
+    // that g^6 stays finite in FP32 (NaN passes through)
+    float gf = (float)(g > 1e5 ? 1e5 : g);
+    float v = gf * root6_f32((float)one_plus_cw3_6 / (powi6<float>(gf) + (float)cw3_6));
+    return g > 1e5 ? (float)fw_lim : v;
 }
 
 // source::compute for one cell (source.rs:55-85), before the factor V.
