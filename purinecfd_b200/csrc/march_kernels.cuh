@@ -614,7 +614,11 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     nxr3 = jst_shfl_down(nx2[0], 1);
                     nyr3 = jst_shfl_down(ny2[0], 1);
                 }
-                if (out_lane) {
+                // With PIPE every lane computes the update (the row buffer holds
+                // the inputs of all 32 lanes, wrapped columns for the halo
+                // lanes) and only the output lanes store, so the update is one
+                // straight block; without it only the output lanes load.
+                if (PIPE || out_lane) {
                     const long id = (long)m * nj + gj;
                     T R[5];
                     for (int v = 0; v < 5; ++v) R[v] = (ftn[v] - ft[v]) + (fnr[v] - fn[v]);
@@ -627,42 +631,39 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                             T a0 = FIRST ? UA(1, v) : (PIPE ? B->uacc[v][lane] : ld(I.uc[0] + v * np + id));
                             T nv = a0 - R[v] * (T)sc;
                             un[v] = (double)nv;
-                            dst[v * np + id] = (TD)nv;
+                            if (out_lane) dst[v * np + id] = (TD)nv;
                         } else {
                             double uo = PIPE ? B->un[v][lane] : I.un[0][v * np + id];
                             if (v == 0) uo0 = uo;
                             if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
                             else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
-                            dst[v * np + id] = (TD)un[v];
-                            if (LAST && sizeof(T) != sizeof(double)) I.uc[0][v * np + id] = (T)un[v];
+                            if (out_lane) dst[v * np + id] = (TD)un[v];
+                            if (LAST && sizeof(T) != sizeof(double) && out_lane) I.uc[0][v * np + id] = (T)un[v];
                         }
                     }
-                    // unpack checks (solver.rs:160-171), on the stored precision
+                    // unpack checks (solver.rs:160-171), on the stored precision;
+                    // the primitives are formed whether or not rho passed (the
+                    // values of a failed cell are not used)
                     bool bad;
                     Prim<double> q{};
                     if (sizeof(T) == sizeof(double)) {
                         double rho = un[0];
-                        bad = isnan(rho) || rho <= 1e-15;
-                        if (!bad) {
-                            q = unpack_cell<double, true>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
-                            bad = isnan(q.p) || q.p <= 1e-15;
-                        }
+                        q = unpack_cell<double, true>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
+                        bad = isnan(rho) || rho <= 1e-15 || isnan(q.p) || q.p <= 1e-15;
                     } else {
                         T rho = (T)un[0];
-                        bad = isnan(rho) || rho <= T(1e-15);
-                        if (!bad) {
-                            Prim<T> qt = unpack_cell<T, true>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], gm1, rgas);
-                            bad = isnan(qt.p) || qt.p <= T(1e-15);
-                            q.vx = qt.vx;
-                            q.vy = qt.vy;
-                            q.t = qt.t;
-                        }
+                        Prim<T> qt = unpack_cell<T, true>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], gm1, rgas);
+                        bad = isnan(rho) || rho <= T(1e-15) || isnan(qt.p) || qt.p <= T(1e-15);
+                        q.vx = qt.vx;
+                        q.vy = qt.vy;
+                        q.t = qt.t;
                     }
-                    if (bad) {
-                        atomicMin(&I.st->bad, (stage_id << 32) | (unsigned long long)id);
-                    } else if (LAST) {
+                    bad = bad && out_lane;
+                    if (bad) atomicMin(&I.st->bad, (stage_id << 32) | (unsigned long long)id);
+                    if (LAST) {
+                        const bool ok = out_lane && !bad;
                         double d = un[0] - uo0;  // solver.rs:195
-                        sres += d * d;
+                        sres += ok ? d * d : 0.0;
                         // timestep.rs:30-42 in the stage arithmetic
                         T aa = T(0.5) * (tx[0] + tx[1]);
                         T bb = T(0.5) * (ty[0] + ty[1]);
@@ -671,9 +672,11 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         T vol = PIPE ? B->volm[lane] : ld(I.mg + MG_N * (id + nj) + MG_VOL);
                         T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
                         T dl = local_dt<T, true>(qvx, qvy, sq<T, true>((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
-                        ratio_next[id] = dv<T, true>(vol, dl);
-                        if (dt_local) I.ldt[id] = (double)dl;
-                        mloc = fmin(mloc, (double)dl);
+                        if (ok) {
+                            ratio_next[id] = dv<T, true>(vol, dl);
+                            if (dt_local) I.ldt[id] = (double)dl;
+                        }
+                        mloc = ok ? fmin(mloc, (double)dl) : mloc;
                     }
                 }
             }
