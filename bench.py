@@ -482,7 +482,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--batch-instances", type=int, default=256, help="config-4 batch size (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=1000, help="step cap per batched instance")
-    ap.add_argument("--plain-instances", type=int, default=8, help="FP64 one-at-a-time subsample")
+    ap.add_argument("--plain-instances", type=int, default=32, help="FP64 one-at-a-time subsample")
     ap.add_argument("--serve", action="store_true", help="run the serving sweep instead of the benchmark")
     ap.add_argument("--serve-rates", default="1,10,50,200")
     ap.add_argument("--serve-requests", type=int, default=64)

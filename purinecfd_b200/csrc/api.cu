@@ -317,23 +317,18 @@ jst_status jst_create(const char* config_json, const double* xy_in, int n_rings,
         g_create_error = "simulation.IM must be >= 3: the JST pressure sensor needs three ghost layers";
         return JST_ERR_CONFIG;
     }
-    // trim_closing_duplicate (mesh.rs:169-189) on the node array
-    std::vector<double> xy(xy_in, xy_in + 2 * (size_t)n_rings * n_theta);
+    // trim_closing_duplicate (mesh.rs:169-189), tested on the caller's node
+    // array; the upload below leaves the duplicate column out (a pitched copy),
+    // so the nodes are not copied on the host
+    const int n_theta_in = n_theta;
     if (n_theta >= 2) {
         bool closed = true;
         for (long r = 0; r < n_rings && closed; ++r) {
-            double ax = xy[2 * (r * n_theta)], ay = xy[2 * (r * n_theta) + 1];
-            double bx = xy[2 * (r * n_theta + n_theta - 1)], by = xy[2 * (r * n_theta + n_theta - 1) + 1];
-            closed = std::fabs(ax - bx) <= 1e-10 && std::fabs(ay - by) <= 1e-10;
+            const double* a = xy_in + 2 * (r * n_theta);
+            const double* b = a + 2 * (n_theta - 1);
+            closed = std::fabs(a[0] - b[0]) <= 1e-10 && std::fabs(a[1] - b[1]) <= 1e-10;
         }
-        if (closed) {
-            int nn = n_theta - 1;
-            std::vector<double> t(2 * (size_t)n_rings * nn);
-            for (long r = 0; r < n_rings; ++r)
-                std::memcpy(&t[2 * (size_t)r * nn], &xy[2 * (size_t)r * n_theta], sizeof(double) * 2 * nn);
-            xy.swap(t);
-            n_theta = nn;
-        }
+        if (closed) n_theta -= 1;
     }
     if (n_rings < 4 || n_theta < 8) {
         g_create_error = "mesh too small: the JST 4th-order stencil needs at least 4 rings and 8 circumferential points";
@@ -358,11 +353,10 @@ jst_status jst_create(const char* config_json, const double* xy_in, int n_rings,
     C.local_dt = o.dt_mode == JST_DT_LOCAL ? 1 : 0;
     C.iteration = raw.iteration;
     C.targetres = raw.targetres;
-    C.nodes = xy;
     double xmin = 1e300, xmax = -1e300;
     for (int t = 0; t < n_theta; ++t) {
-        xmin = std::min(xmin, xy[2 * t]);
-        xmax = std::max(xmax, xy[2 * t]);
+        xmin = std::min(xmin, xy_in[2 * t]);
+        xmax = std::max(xmax, xy_in[2 * t]);
     }
     C.chord = raw.chord > 0.0 ? raw.chord : xmax - xmin;
 
@@ -377,7 +371,7 @@ jst_status jst_create(const char* config_json, const double* xy_in, int n_rings,
     size_t ncell = (size_t)C.ni * C.nj, ntau = (size_t)(C.ni + 1) * C.nj;
     size_t geom_elems = 6 * ncell + 4 * ntau + 4 * ncell;
     if (cudaMalloc(&C.geom_arena, geom_elems * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&C.d_xy, xy.size() * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&C.d_xy, 2 * (size_t)n_rings * n_theta * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&C.d_scratch, 64 * sizeof(double)) != cudaSuccess) {
         g_create_error = "cudaMalloc failed for geometry";
         return JST_ERR_OOM;
@@ -400,7 +394,11 @@ jst_status jst_create(const char* config_json, const double* xy_in, int n_rings,
     g.nny = q; q += ncell;
     g.nmx = q; q += ncell;
     g.nmy = q; q += ncell;
-    cudaMemcpyAsync(C.d_xy, xy.data(), xy.size() * sizeof(double), cudaMemcpyHostToDevice, C.st);
+    if (cudaMemcpy2DAsync(C.d_xy, 2 * sizeof(double) * n_theta, xy_in, 2 * sizeof(double) * n_theta_in,
+                          2 * sizeof(double) * n_theta, n_rings, cudaMemcpyHostToDevice, C.st) != cudaSuccess) {
+        g_create_error = "mesh upload failed";
+        return JST_ERR_CUDA;
+    }
     geometry_build(C.d_xy, n_rings, n_theta, g, C.st);
 
     if (o.kernel_path == JST_PATH_PASSES) {

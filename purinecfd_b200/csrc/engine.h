@@ -24,7 +24,6 @@ struct SolverCore {
     long iteration = 10000;
     double targetres = 1e-10;
     double chord = 1.0;
-    std::vector<double> nodes;  // trimmed, (x,y) interleaved
     cudaStream_t st = nullptr;
     Geom g{};
     double* geom_arena = nullptr;
