@@ -222,12 +222,15 @@ JST_HD void euler_flux(const T fu[5], T nx, T ny, T gm1, T out[5], T p_ref = T(0
 template <class T>
 JST_HD void green_gauss(T c, T vup, T vdn, T vlf, T vrt, T upx, T upy, T dnx, T dny, T lfx, T lfy, T rtx, T rty,
                         T inv_v, T* gx, T* gy) {
-    T f_up = T(0.5) * (c + vup);
-    T f_dn = T(0.5) * (c + vdn);
-    T f_lf = T(0.5) * (c + vlf);
-    T f_rt = T(0.5) * (c + vrt);
-    *gx = (f_up * upx - f_dn * dnx + f_rt * rtx - f_lf * lfx) * inv_v;
-    *gy = (f_up * upy - f_dn * dny + f_rt * rty - f_lf * lfy) * inv_v;
+    // the face values' factor 1/2 is applied once, to 1/V: scaling by a
+    // power of two is exact, so the result is bit for bit the reference's
+    T f_up = c + vup;
+    T f_dn = c + vdn;
+    T f_lf = c + vlf;
+    T f_rt = c + vrt;
+    T h = T(0.5) * inv_v;
+    *gx = (f_up * upx - f_dn * dnx + f_rt * rtx - f_lf * lfx) * h;
+    *gy = (f_up * upy - f_dn * dny + f_rt * rty - f_lf * lfy) * h;
 }
 
 // The same Green-Gauss sum in difference form, sum_f 0.5 (phi_nb - phi_c) n_f / V:
@@ -236,12 +239,13 @@ JST_HD void green_gauss(T c, T vup, T vdn, T vlf, T vrt, T upx, T upy, T dnx, T 
 template <class T>
 JST_HD void green_gauss_delta(T c, T vup, T vdn, T vlf, T vrt, T upx, T upy, T dnx, T dny, T lfx, T lfy, T rtx,
                               T rty, T inv_v, T* gx, T* gy) {
-    T d_up = T(0.5) * (vup - c);
-    T d_dn = T(0.5) * (vdn - c);
-    T d_lf = T(0.5) * (vlf - c);
-    T d_rt = T(0.5) * (vrt - c);
-    *gx = (d_up * upx - d_dn * dnx + d_rt * rtx - d_lf * lfx) * inv_v;
-    *gy = (d_up * upy - d_dn * dny + d_rt * rty - d_lf * lfy) * inv_v;
+    T d_up = vup - c;
+    T d_dn = vdn - c;
+    T d_lf = vlf - c;
+    T d_rt = vrt - c;
+    T h = T(0.5) * inv_v;  // as in green_gauss
+    *gx = (d_up * upx - d_dn * dnx + d_rt * rtx - d_lf * lfx) * h;
+    *gy = (d_up * upy - d_dn * dny + d_rt * rty - d_lf * lfy) * h;
 }
 
 // Diffusion tensor columns of one cell (viscous.rs:37-71): returns mu, chi,
