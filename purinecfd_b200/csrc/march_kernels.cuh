@@ -77,10 +77,14 @@ JST_D f2 f2_mul(f2 a, f2 b) { return f2{a.x * b.x, a.y * b.y}; }
 #endif
 JST_D f2 f2_splat(float a) { return f2_make(a, a); }
 
-// Net face flux out = cv - vis - lam (d1 e2 - d3 e4) of the five components,
-// with d1 = w2 - w1 and d3 = w3 - 3 w2 + 3 w1 - w0 (w0..w3 the states at
-// face-2 .. face+1) and vis = (dA + dB) hx + (dA' + dB') hy from the two
-// cells' diffusion tensors (components 1-4; component 0 has none).
+// Net face flux out = cv2 / 2 - vis - lam (d1 e2 - d3 e4) of the five
+// components, with d1 = w2 - w1 and d3 = w3 - 3 w2 + 3 w1 - w0 (w0..w3 the
+// states at face-2 .. face+1) and vis = (dA + dB) hx + (dA' + dB') hy from the
+// two cells' diffusion tensors (components 1-4; component 0 has none).  cv2
+// is the convective flux of twice the face state w1 + w2: the Euler flux is
+// homogeneous of degree one in U and scaling by 2 is exact, so cv2 / 2 is bit
+// for bit the flux of (w1 + w2) / 2 (convection.rs:55, 64), one multiply per
+// component fewer.
 template <class T>
 JST_D void face_combine(const T* w0, const T* w1, const T* w2, const T* w3, const T* cv, const T* dA, const T* dB,
                         T hx, T hy, T lam, T e2, T e4, T* out) {
@@ -88,10 +92,10 @@ JST_D void face_combine(const T* w0, const T* w1, const T* w2, const T* w3, cons
         {  // component 0
             T d1 = w2[0] - w1[0];
             T d3 = w3[0] - T(3) * w2[0] + T(3) * w1[0] - w0[0];
-            out[0] = cv[0] - lam * (d1 * e2 - d3 * e4);
+            out[0] = T(0.5) * cv[0] - lam * (d1 * e2 - d3 * e4);
         }
-        const f2 m1 = f2_splat(-1.0f), m3 = f2_splat(-3.0f), p3 = f2_splat(3.0f);
-        const f2 hx2 = f2_splat(hx), hy2 = f2_splat(hy), e22 = f2_splat(e2), me42 = f2_splat(-e4);
+        const f2 m1 = f2_splat(-1.0f), m3 = f2_splat(-3.0f), p3 = f2_splat(3.0f), half = f2_splat(0.5f);
+        const f2 mhx2 = f2_splat(-hx), mhy2 = f2_splat(-hy), e22 = f2_splat(e2), me42 = f2_splat(-e4);
         const f2 mlam = f2_splat(-lam);
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -102,9 +106,9 @@ JST_D void face_combine(const T* w0, const T* w1, const T* w2, const T* w3, cons
             f2 D3 = f2_fma(W0, m1, f2_fma(W1, p3, f2_fma(W2, m3, W3)));
             f2 DX = f2_add(f2_make(dA[a - 1], dA[b - 1]), f2_make(dB[a - 1], dB[b - 1]));
             f2 DY = f2_add(f2_make(dA[a + 3], dA[b + 3]), f2_make(dB[a + 3], dB[b + 3]));
-            f2 VIS = f2_fma(DX, hx2, f2_mul(DY, hy2));
+            f2 NVIS = f2_fma(DX, mhx2, f2_mul(DY, mhy2));
             f2 DIS = f2_fma(D3, me42, f2_mul(D1, e22));
-            f2 O = f2_fma(DIS, mlam, f2_fma(VIS, m1, f2_make(cv[a], cv[b])));
+            f2 O = f2_fma(DIS, mlam, f2_fma(f2_make(cv[a], cv[b]), half, NVIS));
             f2_split(O, out[a], out[b]);
         }
     } else {
@@ -114,7 +118,7 @@ JST_D void face_combine(const T* w0, const T* w1, const T* w2, const T* w3, cons
             T d3 = w3[v] - T(3) * w2[v] + T(3) * w1[v] - w0[v];
             T vis = T(0);
             if (v > 0) vis = (dA[v - 1] + dB[v - 1]) * hx + (dA[v + 3] + dB[v + 3]) * hy;
-            out[v] = cv[v] - vis - lam * (d1 * e2 - d3 * e4);
+            out[v] = (T(0.5) * cv[v] - vis) - lam * (d1 * e2 - d3 * e4);
         }
     }
 }
@@ -304,7 +308,9 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         const bool out_lane = lane >= 3 && lane < 3 + MARCH_W && cu < nj;
         const T gm1 = (T)c.gm1, rgas = (T)c.r_gas;
         const T half_cfl = (T)c.half_cfl, k2 = (T)c.k2, k4 = (T)c.k4;
-        const T p_ref = sizeof(T) == sizeof(double) ? T(0) : (T)c.p_inf;  // see euler_flux
+        // face fluxes are formed from twice the face state (see face_combine),
+        // so the pressure reference of euler_flux is doubled as well
+        const T p_ref2 = sizeof(T) == sizeof(double) ? T(0) : (T)(2.0 * c.p_inf);
 
         // PIPE: stage the global inputs that row kk of the walk reads.  The
         // conditions are the ones under which the walk reads them.
@@ -574,10 +580,10 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     w1[v] = UA(1, v);
                     w2[v] = UA(2, v);
                     w3[v] = UA(3, v);
-                    fu[v] = T(0.5) * (w1[v] + w2[v]);
+                    fu[v] = w1[v] + w2[v];
                 }
                 const T fnx = tx[1], fny = ty[1];
-                euler_flux<T, true>(fu, fnx, fny, gm1, cv, p_ref);
+                euler_flux<T, true>(fu, fnx, fny, gm1, cv, p_ref2);
                 T hx = T(0.5) * fnx, hy = T(0.5) * fny;
                 face_combine<T>(w0, w1, w2, w3, cv, dw[0], dw[1], hx, hy, lam, e2, e4, ftn);
             }
@@ -599,9 +605,9 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         ul1[v] = jst_shfl_up(um[v], 1);
                         ul2[v] = jst_shfl_up(um[v], 2);
                         ur1[v] = jst_shfl_down(um[v], 1);
-                        fu[v] = T(0.5) * (ul1[v] + um[v]);
+                        fu[v] = ul1[v] + um[v];
                     }
-                    euler_flux<T, true>(fu, nx2[0], ny2[0], gm1, cv, p_ref);
+                    euler_flux<T, true>(fu, nx2[0], ny2[0], gm1, cv, p_ref2);
                     T hx = T(0.5) * nx2[0], hy = T(0.5) * ny2[0];
                     T dl[8];
                     for (int v = 0; v < 8; ++v) dl[v] = jst_shfl_up(dw[0][v], 1);
