@@ -147,6 +147,35 @@ def test_fused_set_conserved_nonphysical():
     assert (ei.value.i, ei.value.j, ei.value.rho) == (3, 7, -2.0)
 
 
+@pytest.mark.parametrize("path", ["strips", "tiles", "passes"])
+@pytest.mark.parametrize("case", [("fangdata", 20.0), ("ellipse", 50.0)], ids=lambda c: f"{c[0]}-cfl{c[1]:g}")
+def test_first_failed_cell_matches_oracle(path, case):
+    """At a CFL where the first step already fails, the reported cell is the
+    oracle's: the first failing cell in row-major order of the first stage with
+    one (solver.rs:160-171) — (0, 5) on fangdata at CFL 20, not (0, 0) — with
+    its density and pressure."""
+    from purinecfd_b200 import PATH_PASSES, NonPhysical, Solver, meshgen
+    name, cfl = case
+    if name == "fangdata":
+        xy, nr, nt = mesh_case("fangdata.txt")
+    else:
+        nr, nt = 13, 40
+        xy = meshgen.ellipse_o_mesh(nr, nt)
+    cfg = load_config({"simulation": {"CFL": cfl}})
+    o = jo.OracleSolver(cfg, xy, nr, nt)
+    with pytest.raises(FloatingPointError):
+        o.advance()
+    oi, oj, orho, op = o.nonphysical()
+    kw = {"strips": dict(tile_i=8, tile_j=26, block_threads=64), "tiles": dict(tile_i=8, tile_j=32, block_threads=256)}
+    s = Solver(cfg, xy, nr, nt, kernel_path=PATH_PASSES) if path == "passes" else _solver(cfg, xy, nr, nt, **kw[path])
+    with pytest.raises(NonPhysical) as ei:
+        s.advance()
+    e = ei.value
+    assert (e.i, e.j) == (oi, oj)
+    assert abs(e.rho - orho) <= 1e-8 * abs(orho)
+    assert (np.isnan(e.p) and np.isnan(op)) or abs(e.p - op) <= 1e-6 * abs(op)
+
+
 def test_forces_agree_across_paths_and_oracle():
     """CL/CD (no counterpart in the reference) from the fused path, the passes
     path and the oracle's wall-force integrator agree on the same state."""
