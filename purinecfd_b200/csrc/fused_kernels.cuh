@@ -612,10 +612,10 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
             }
         }
         int o = li * LJ + lj;
-        Diff<T> d = diffusion_tensor<T, true>(sQ[2 * NL + o], sU[4 * NL + o], sQ[0 * NL + o], sQ[1 * NL + o], g[0], g[1],
-                                        g[2], g[3], g[4], g[5], g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num,
-                                        (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp,
-                                        (T)c.sigma);
+        Diff<T> d = diffusion_tensor<T, true>(sQ[2 * NL + o], sU[4 * NL + o], sQ[0 * NL + o], sQ[1 * NL + o],
+                                              g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], (T)c.inv_t_ref,
+                                              (T)c.suth_num, (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr,
+                                              (T)c.inv_prt, (T)c.cp, (T)c.sigma);
         sD[0 * NR + w] = d.dx1;
         sD[1 * NR + w] = d.dx2;
         sD[2 * NR + w] = d.dx3;
@@ -626,7 +626,8 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
         sD[7 * NR + w] = d.dy4;
         if (ri >= 1 && ri <= TI && rj >= 1 && rj <= TJ) {
             int tcell = (ri - 1) * TJ + (rj - 1);
-            T s5 = sa_source<T, true>(sU[o], sU[4 * NL + o], (T)gs[L::gD2 + tcell], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
+            T s5 = sa_source<T, true>(sU[o], sU[4 * NL + o], (T)gs[L::gD2 + tcell], d.chi, d.fv1, g[2], g[1], g[6],
+                                      g[7], c);
             sS[tcell] = s5 * (T)gs[L::gV + tcell];
         }
     }

@@ -508,9 +508,10 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                             green_gauss_delta<T>(cq, qk[q], qw[0][q], lf, rg, txk, tyk, tx[2], ty[2], nxr, nyr, rtx,
                                                  rty, iv, &g[2 * q], &g[2 * q + 1]);
                     }
-                    Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], g[0], g[1], g[2], g[3], g[4],
-                                                    g[5], g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num, (T)c.t_suth,
-                                                    (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp, (T)c.sigma);
+                    Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], g[0], g[1], g[2],
+                                                          g[3], g[4], g[5], g[6], g[7], (T)c.inv_t_ref,
+                                                          (T)c.suth_num, (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr,
+                                                          (T)c.inv_prt, (T)c.cp, (T)c.sigma);
                     dn[0] = d.dx1;
                     dn[1] = d.dx2;
                     dn[2] = d.dx3;
@@ -520,16 +521,17 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     dn[6] = d.dy3;
                     dn[7] = d.dy4;
                     if (S || (r >= i0 && r < i1)) {
-                        T s5 = sa_source<T, true>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], c);
+                        T s5 = sa_source<T, true>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6],
+                                                  g[7], c);
                         snew = s5 * gk[MG_VOL];
                     }
                     if (!S && r == 0) {
                         // the wall ghost ring (row -1, one row up in the window) takes cell
                         // 0's gradient with grad T = 0 (gradient.rs:93-95)
-                        Diff<T> w = diffusion_tensor<T, true>(qw[0][2], UA(2, 4), qw[0][0], qw[0][1], g[0], g[1], g[2], g[3],
-                                                        T(0), T(0), g[6], g[7], (T)c.inv_t_ref, (T)c.suth_num,
-                                                        (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt,
-                                                        (T)c.cp, (T)c.sigma);
+                        Diff<T> w = diffusion_tensor<T, true>(qw[0][2], UA(2, 4), qw[0][0], qw[0][1], g[0], g[1],
+                                                              g[2], g[3], T(0), T(0), g[6], g[7], (T)c.inv_t_ref,
+                                                              (T)c.suth_num, (T)c.t_suth, (T)c.cv1_cubed,
+                                                              (T)c.inv_pr, (T)c.inv_prt, (T)c.cp, (T)c.sigma);
                         dw[1][0] = w.dx1;
                         dw[1][1] = w.dx2;
                         dw[1][2] = w.dx3;
@@ -540,10 +542,10 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         dw[1][7] = w.dy4;
                     }
                 } else if (r >= ni) {  // far ghost ring: zero gradient (gradient.rs:96)
-                    Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], T(0), T(0), T(0), T(0),
-                                                    T(0), T(0), T(0), T(0), (T)c.inv_t_ref, (T)c.suth_num,
-                                                    (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr, (T)c.inv_prt, (T)c.cp,
-                                                    (T)c.sigma);
+                    Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], T(0), T(0), T(0),
+                                                          T(0), T(0), T(0), T(0), T(0), (T)c.inv_t_ref,
+                                                          (T)c.suth_num, (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr,
+                                                          (T)c.inv_prt, (T)c.cp, (T)c.sigma);
                     dn[0] = d.dx1;
                     dn[1] = d.dx2;
                     dn[2] = d.dx3;
