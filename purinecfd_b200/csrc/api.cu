@@ -17,6 +17,7 @@
 #include <memory>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/jst_gpu.h"
@@ -518,10 +519,31 @@ jst_status jst_step_count(const jst_solver* s, int64_t* out) {
     return JST_OK;
 }
 
+// Touches every page of a large output buffer from several threads before a
+// device-to-host copy into it.  A freshly allocated host array is mapped on
+// first write, and the kernel zero-fills each new page on the faulting
+// thread; done inside the copy that runs on one thread at a few GB/s (on a
+// 4.2 M-cell field, 9 ms of a copy that takes 2 ms into mapped memory).
+static void prefault(void* p, size_t bytes) {
+    constexpr size_t kPage = 4096, kMin = size_t(4) << 20;
+    if (bytes < kMin) return;
+    const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t per = (bytes + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t)
+        th.emplace_back([=] {
+            volatile char* c = static_cast<volatile char*>(p);
+            const size_t a = t * per, b = std::min(bytes, a + per);
+            for (size_t k = a; k < b; k += kPage) c[k] = 0;
+        });
+    for (auto& x : th) x.join();
+}
+
 jst_status jst_get_field(jst_solver* s, int field, double* out, size_t n) {
     if (!s || !out || field < 0 || field >= JST_F_COUNT) return JST_ERR_ARG;
     size_t nc = (size_t)s->core.ni * s->core.nj;
     if (n < nc) return JST_ERR_ARG;
+    prefault(out, nc * sizeof(double));
     const Geom& g = s->core.g;
     const double* geo = nullptr;
     switch (field) {
