@@ -309,6 +309,7 @@ def run_ours(args, world, rank, local):
                                                "bytes_per_cell_stage": b64,
                                                "kernel": "x".join(map(str, s64.kernel_config()))}}
             s64.close()
+            line["split_vs_fp64"] = split_vs_fp64(cfg, xy, nr, nt, local)
         # end to end through the public API from host buffers: create (mesh H2D,
         # geometry on the GPU), K steps with the per-step residual read back,
         # final fields D2H
@@ -340,6 +341,26 @@ def run_ours(args, world, rank, local):
                                     "sample": f"{args.workload}: {r['cells']} cells, 1 untimed + 2 timed RK steps, "
                                               f"oracle (CPU FP64 restatement of jst-rs), {r['cores']} threads"}
         print(json.dumps(line), flush=True)
+
+
+def split_vs_fp64(cfg, xy, nr, nt, device, steps: int = 100) -> dict:
+    """Error of the FP32/FP64 split path against the FP64 path (itself within
+    1e-13 of the oracle on the parity workloads) on this workload: both run the
+    same steps from the initial state; per field, the largest difference
+    relative to the field's scale, and the CL/CD differences."""
+    from purinecfd_b200 import PATH_FUSED, PREC_FP32_SPLIT, PREC_FP64, Solver
+    runs = []
+    for prec in (PREC_FP32_SPLIT, PREC_FP64):
+        s = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=device)
+        s.run(steps)
+        runs.append(({f: s.get(f) for f in ("rho", "p", "T", "u", "v", "nut")}, s.forces()))
+        s.close()
+    (fa, (cla, cda)), (fb, (clb, cdb)) = runs
+    err = {}
+    for f in fa:
+        scale = float(np.max(np.abs(fb[f]))) or 1.0
+        err[f] = float(f"{float(np.max(np.abs(fa[f] - fb[f]))) / scale:.3g}")
+    return {"steps": steps, "field_err_rel_scale": err, "cl_fp64": clb, "dcl": abs(cla - clb), "dcd": abs(cda - cdb)}
 
 
 def batched_leg(args, world: int = 1, rank: int = 0):
