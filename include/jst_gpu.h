@@ -26,8 +26,8 @@ typedef struct jst_solver jst_solver;
 
 /* Status codes.  The JST_ERR_MESH_* values map one-to-one onto the
  * reference's MeshError variants (mesh.rs:17-44); JST_ERR_CONFIG is its
- * io::Error(InvalidData) from Config::from_str (config.rs:243-248);
- * JST_ERR_NONPHYSICAL is NonPhysical (state.rs:589-606). */
+ * io::Error(InvalidData) from Config::from_str (config.rs:165-170);
+ * JST_ERR_NONPHYSICAL is NonPhysical (state.rs:242-257). */
 typedef enum {
     JST_OK = 0,
     JST_ERR_MESH_IO = 1,
@@ -103,7 +103,7 @@ const char* jst_last_error(const jst_solver* s);
 int jst_ni(const jst_solver* s);
 int jst_nj(const jst_solver* s);
 
-/* The NonPhysical error of state.rs:589-606. */
+/* The NonPhysical error of state.rs:242-257. */
 typedef struct {
     int64_t i, j;
     double rho, p;
@@ -137,6 +137,17 @@ jst_status jst_run(jst_solver* s, int64_t max_steps, jst_step_cb cb, void* user,
  * when *dt is non-NULL (timestep::compute, timestep.rs:24-47), returning the
  * global minimum in *dt. */
 jst_status jst_residual_terms(jst_solver* s, double* dt);
+
+/* The residual the RK update applies (solver.rs:128-133), R = Fc - Fv - Fd
+ * with S subtracted from component 4, of every interior cell of the current
+ * state: Solver::residual_terms (solver.rs:86-94) after timestep::compute
+ * (timestep.rs:24-47), combined per cell.  On the fused path R comes from
+ * the stage kernel this solver runs its RK stages with (the autotuned
+ * marching-strip or tile kernel, in the solver's precision; stage 0 run
+ * without its update); on the passes path from the separate terms.  out
+ * receives 5 planes of NI*NJ doubles (component-major, i-major / j-minor);
+ * n >= 5*NI*NJ.  The conserved state is not changed. */
+jst_status jst_stage_residual(jst_solver* s, double* out, size_t n);
 
 /* timestep::compute (timestep.rs:24-57) on the current state. */
 jst_status jst_timestep(jst_solver* s, double* dt);
@@ -283,9 +294,13 @@ jst_status jst_batch_result_get(jst_batch* b, int64_t id, jst_batch_result* r, d
  * stream) and returns without synchronising or allocating.  Its scratch is a
  * fixed file-scope device array of 8192 partial sums, so NI*NJ may not exceed
  * 16,777,216 cells (larger sizes fail with JST_ERR_ARG before any launch).
- * The first call on a device looks up that array's address; make it before
- * any stream capture.  All calls share the array: calls whose kernels overlap
- * on the GPU race, so serialise them (one stream, or events). */
+ * The kernels run on the calling thread's current device (cudaSetDevice),
+ * whatever device the pointers belong to, so make the fields' device current
+ * first.  The first call in each CUDA context on a device looks up that
+ * array's address (again after cudaDeviceReset, which creates a new
+ * context); make it before any stream capture.  All calls share the array:
+ * calls whose kernels overlap on the GPU race, so serialise them (one
+ * stream, or events). */
 jst_status jst_residual_noalloc(const double* rho, const double* rho_prev, int ni, int nj, double* out,
                                 void* stream);
 

@@ -17,7 +17,7 @@
 // Citations are file:line within the reference's jst-rs/ crate.
 //
 // Additions that the reference does not have (marked "EXT"): an optional
-// free-stream nu-tilde ratio (the reference hard-codes 0.1, config.rs:274),
+// free-stream nu-tilde ratio (the reference hard-codes 0.1, config.rs:196),
 // an opt-in local time stepping mode, and a wall-force (CL/CD) integrator.
 // With their defaults the restatement is the reference's algorithm unchanged.
 
@@ -38,7 +38,7 @@
 namespace {
 
 // ---------------------------------------------------------------- config ----
-// config.rs:88-189 (inputs) and config.rs:191-223 (derived constants).
+// config.rs:11-111 (inputs) and config.rs:115-145, 173-206 (derived constants).
 struct Config {
     double gamma, r_gas, t_ref, t_suth, mu0;
     double aoa, mach, cfl;
@@ -48,7 +48,7 @@ struct Config {
     double targetres;
     double Cv1, Pr, Prt, sigma, Cb1, Cb2, Ct3, Ct4, Cw2, Cw3, fv3, kappa, rmax;
     double k2, k4;
-    double nut_ratio;  // EXT: 0.1 in the reference (config.rs:274)
+    double nut_ratio;  // EXT: 0.1 in the reference (config.rs:196)
     int local_dt;      // EXT: 0 = global minimum step (solver.rs:110-116)
 
     double cv, cp, cw1, cv1_cubed, c_inf, u_inf, v_inf, rho_inf, mu_inf, nut_inf;
@@ -66,13 +66,13 @@ inline double powi6(double x) {
     return x2 * x4;
 }
 
-// config.rs:230-234
+// config.rs:153-156
 double sutherland(double mu0, double t, double t_ref, double t_suth) {
     double r = t / t_ref;
     return mu0 * (r * std::sqrt(r)) * (t_ref + t_suth) / (t + t_suth);
 }
 
-// config.rs:251-284
+// config.rs:173-206
 void finish(Config& c) {
     double cv = c.r_gas / (c.gamma - 1.0);
     double c_inf = std::sqrt(c.gamma * c.r_gas * c.t_inf);
@@ -101,13 +101,13 @@ void finish(Config& c) {
     c.one_plus_cw3_6 = 1.0 + powi6(c.Cw3);
 }
 
-// config.rs:287-291
+// config.rs:210-213
 inline double mu_of(const Config& c, double t) {
     double r = t * c.inv_t_ref;
     return r * std::sqrt(r) * c.suth_num / (t + c.t_suth);
 }
 
-const double RK_ALPHA[5] = {0.25, 1.0 / 6.0, 0.375, 0.5, 1.0};  // config.rs:295
+const double RK_ALPHA[5] = {0.25, 1.0 / 6.0, 0.375, 0.5, 1.0};  // config.rs:217
 
 // ----------------------------------------------------------------- field ----
 // Halo-indexed row-major storage, i slow / j fast (field.rs:139-192).
@@ -161,7 +161,7 @@ struct Solver {
     double totaltime = 0.0;
     long step = 0;
 
-    // Non-physical report of the last failing unpack (state.rs:589-596).
+    // Non-physical report of the last failing unpack (state.rs:242-257).
     long bad_i = 0, bad_j = 0;
     double bad_rho = 0.0, bad_p = 0.0;
 
@@ -262,7 +262,7 @@ struct Prim {
     double rho, p, t, vx, vy, e, h, c, nut;
 };
 
-// state.rs:569-587
+// state.rs:222-237
 Prim from_primitives(const Config& c, double rho, double vx, double vy, double p, double nut) {
     double gamma = c.gamma;
     double t = p / (c.r_gas * rho);
@@ -280,7 +280,7 @@ Prim from_primitives(const Config& c, double rho, double vx, double vy, double p
     return s;
 }
 
-// state.rs:490-505
+// state.rs:143-156
 inline void pack(Solver& s, long i, long j) {
     double r = s.rho(i, j);
     s.U[0](i, j) = r;
@@ -290,7 +290,7 @@ inline void pack(Solver& s, long i, long j) {
     s.U[4](i, j) = r * s.nut(i, j);
 }
 
-// state.rs:507-520
+// state.rs:160-171
 inline void write_state(Solver& s, long i, long j, const Prim& q) {
     s.rho(i, j) = q.rho;
     s.p(i, j) = q.p;
@@ -304,7 +304,7 @@ inline void write_state(Solver& s, long i, long j, const Prim& q) {
     pack(s, i, j);
 }
 
-// state.rs:522-539
+// state.rs:174-190
 void initialize(Solver& s) {
     const Config& c = s.cfg;
     Prim q = from_primitives(c, c.p_inf / (c.r_gas * c.t_inf), c.u_inf, c.v_inf, c.p_inf, c.nut_inf);
@@ -318,7 +318,7 @@ void initialize(Solver& s) {
         }
 }
 
-// state.rs:547-552 — every addressable cell, halo and corners included.
+// state.rs:198-203 — every addressable cell, halo and corners included.
 void set_uniform(Solver& s, double rho, double vx, double vy, double p, double nut) {
     Prim q = from_primitives(s.cfg, rho, vx, vy, p, nut);
     for (long i = -s.H; i < s.ni + s.H; ++i)

@@ -34,10 +34,10 @@ namespace jst {
 // Error text for entry points without a handle (read with jst_last_error(NULL)).
 void set_call_error(const std::string& msg) { g_create_error = msg; }
 
-const double RK_ALPHA[5] = {0.25, 1.0 / 6.0, 0.375, 0.5, 1.0};  // config.rs:295
+const double RK_ALPHA[5] = {0.25, 1.0 / 6.0, 0.375, 0.5, 1.0};  // config.rs:217
 
-// Config::finish (config.rs:251-284) + the constant sub-expressions of
-// PhysConst + the free-stream state of Cells::initialize (state.rs:522-539).
+// Config::finish (config.rs:173-206) + the constant sub-expressions of
+// PhysConst + the free-stream state of Cells::initialize (state.rs:174-190).
 PhysConst make_phys(const RawConfig& r) {
     PhysConst c{};
     c.gamma = r.gamma;
@@ -92,7 +92,7 @@ PhysConst make_phys(const RawConfig& r) {
     c.cb2_sigma = r.Cb2 * r.sigma;
     c.r_gas_gamma = r.r_gas * r.gamma;
     c.halo = (int)r.halo;
-    // PrimState::from_primitives (state.rs:569-587) of the free stream
+    // PrimState::from_primitives (state.rs:222-237) of the free stream
     double rho = r.p_inf / (r.r_gas * r.t_inf);
     double p = r.p_inf;
     double t = p / (r.r_gas * rho);
@@ -107,7 +107,7 @@ PhysConst make_phys(const RawConfig& r) {
     c.f_c = std::sqrt(r.gamma * r.r_gas * t);
     c.f_nut = c.nut_inf;
     double rm = r.t_inf * c.inv_t_ref;
-    c.f_mu = rm * std::sqrt(rm) * c.suth_num / (r.t_inf + r.t_suth);  // Config::mu (config.rs:287-291)
+    c.f_mu = rm * std::sqrt(rm) * c.suth_num / (r.t_inf + r.t_suth);  // Config::mu (config.rs:210-213)
     return c;
 }
 
@@ -177,6 +177,26 @@ class PassesEngine : public Engine {
         }
         passes_residual_terms(P_, core_->g, core_->c, core_->st);
         return cudaStreamSynchronize(core_->st) == cudaSuccess ? JST_OK : JST_ERR_CUDA;
+    }
+
+    // The terms of the passes (time step first, then residual_terms) combined
+    // on the host in the order of Solver::update (solver.rs:128-133).
+    jst_status stage_residual(double* out) override {
+        double dt = 0.0;
+        jst_status rc = residual_terms(&dt);
+        if (rc != JST_OK) return rc;
+        size_t n = (size_t)core_->ni * core_->nj;
+        std::vector<double> fv(n), fd(n);
+        for (int k = 0; k < 5; ++k) {
+            double* r = out + k * n;
+            if (!get_field(JST_F_FC0 + k, r) || !get_field(JST_F_FV0 + k, fv.data()) ||
+                !get_field(JST_F_FD0 + k, fd.data()))
+                return JST_ERR_CUDA;
+            for (size_t q = 0; q < n; ++q) r[q] = r[q] - fv[q] - fd[q];
+        }
+        if (!get_field(JST_F_S, fv.data())) return JST_ERR_CUDA;
+        for (size_t q = 0; q < n; ++q) out[4 * n + q] -= fv[q];
+        return JST_OK;
     }
 
     jst_status timestep(double* dt) override {
@@ -500,6 +520,19 @@ jst_status jst_run(jst_solver* s, int64_t max_steps, jst_step_cb cb, void* user,
 }
 
 jst_status jst_residual_terms(jst_solver* s, double* dt) { return s ? s->eng->residual_terms(dt) : JST_ERR_ARG; }
+
+jst_status jst_stage_residual(jst_solver* s, double* out, size_t n) {
+    if (!s || !out) return JST_ERR_ARG;
+    size_t nc = (size_t)s->core.ni * s->core.nj;
+    if (n < 5 * nc) {
+        s->err = "jst_stage_residual: out must hold 5*NI*NJ doubles";
+        return JST_ERR_ARG;
+    }
+    jst_status rc = s->eng->stage_residual(out);
+    if (rc == JST_ERR_CUDA) return cuda_fail(s, "stage_residual");
+    if (rc == JST_ERR_OOM) s->err = "jst_stage_residual: cudaMalloc failed for the residual buffer";
+    return rc;
+}
 jst_status jst_timestep(jst_solver* s, double* dt) { return s && dt ? s->eng->timestep(dt) : JST_ERR_ARG; }
 
 jst_status jst_residual(jst_solver* s, double* out) {
@@ -524,6 +557,8 @@ jst_status jst_step_count(const jst_solver* s, int64_t* out) {
 // first write, and the kernel zero-fills each new page on the faulting
 // thread; done inside the copy that runs on one thread at a few GB/s (on a
 // 4.2 M-cell field, 9 ms of a copy that takes 2 ms into mapped memory).
+// Each touch writes back the byte it read, so the caller's data is unchanged
+// when the call then fails.
 static void prefault(void* p, size_t bytes) {
     constexpr size_t kPage = 4096, kMin = size_t(4) << 20;
     if (bytes < kMin) return;
@@ -534,7 +569,7 @@ static void prefault(void* p, size_t bytes) {
         th.emplace_back([=] {
             volatile char* c = static_cast<volatile char*>(p);
             const size_t a = t * per, b = std::min(bytes, a + per);
-            for (size_t k = a; k < b; k += kPage) c[k] = 0;
+            for (size_t k = a; k < b; k += kPage) c[k] = c[k];
         });
     for (auto& x : th) x.join();
 }
@@ -720,7 +755,7 @@ jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_m
     return rc;
 }
 
-// Test hooks (not in the public header): uniform state on every cell and a
+// Test hooks (declared in include/jst_gpu_debug.h): uniform state on every cell and a
 // single kernel by name, for the free-stream properties that must bypass the
 // boundary conditions (jst-rs/tests/properties.rs:126-156).
 jst_status jst_debug_set_uniform(jst_solver* s, double rho, double vx, double vy, double p, double nut) {

@@ -1,5 +1,5 @@
 // Host-side readers for the reference's two input formats:
-//  * config.json (jst-rs/src/config.rs:88-189, serde field names and defaults),
+//  * config.json (jst-rs/src/config.rs:11-111, serde field names and defaults),
 //  * the O-mesh text file (jst-rs/src/mesh.rs:109-189).
 // Both return the reference's error cases as status codes plus a message.
 #pragma once
@@ -193,8 +193,8 @@ struct RawConfig {
     double aoa, mach, cfl;
     long halo;
     double t_inf, p_inf;
-    long iteration = 10000;   // config.rs:130-132
-    double targetres = 1e-10; // config.rs:133-135
+    long iteration = 10000;   // config.rs:52-54
+    double targetres = 1e-10; // config.rs:55-57
     double Cv1, Pr, Prt, sigma, Cb1, Cb2, Ct3, Ct4, Cw2, Cw3, fv3, kappa, rmax;
     double k2, k4;
     double nut_inf_ratio = 0.1;  // optional `simulation.nut_inf_ratio`; the reference hard-codes 0.1

@@ -42,6 +42,9 @@ class Engine {
     virtual void init() = 0;
     virtual jst_status advance(jst_nonphysical* bad) = 0;
     virtual jst_status residual_terms(double* dt) = 0;
+    // R = Fc - Fv - Fd, R[4] -= S of every interior cell of the current state
+    // (5 planes of NI*NJ into out, host memory), from the stage kernels
+    virtual jst_status stage_residual(double* out) = 0;
     virtual jst_status timestep(double* dt) = 0;
     virtual bool get_field(int id, double* out) = 0;
     virtual jst_status set_conserved(const double* u5, jst_nonphysical* bad) = 0;

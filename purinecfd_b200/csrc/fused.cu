@@ -34,7 +34,7 @@ using fused::TileRef;
 
 namespace {
 
-// Initial state: U_n = pack(free stream) on every cell (state.rs:522-539).
+// Initial state: U_n = pack(free stream) on every cell (state.rs:174-190).
 __global__ void k_fill_freestream(double* u0, double* u1, double* u2, double* u3, double* u4, long n, PhysConst c) {
     long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
@@ -154,6 +154,8 @@ void launch_wall_force(const Geom& g, const UnPtrs& up, const PhysConst& c, doub
 template <class T> struct Kernels {
     void (*stage[3])(const TileRef*, int*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};
     void (*step_dt)(const TileRef*, const int*, const Inst<T>*, int, int) = nullptr;
+    // stage 0 writing the residual of every cell to Inst::rdump (jst_stage_residual)
+    void (*dump)(const TileRef*, int*, const Inst<T>*, int, double) = nullptr;
     size_t smem = 0;
     int nt = 256;
     bool march = false;  // warp per work item (else block per tile)
@@ -164,6 +166,7 @@ template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
     k.stage[0] = fused::k_stage<T, TI, TJ, NT, true, false>;
     k.stage[1] = fused::k_stage<T, TI, TJ, NT, false, false>;
     k.stage[2] = fused::k_stage<T, TI, TJ, NT, false, true>;
+    k.dump = fused::k_stage<T, TI, TJ, NT, true, false, true>;
     k.step_dt = fused::k_step_dt<T, NT>;
     k.smem = fused::Layout<T, TI, TJ, NT>::bytes;
     k.nt = NT;
@@ -176,6 +179,7 @@ template <class T, int NT> Kernels<T> march_kernels_for() {
     k.stage[0] = fused::k_march<T, NT, true, false, PIPE>;
     k.stage[1] = fused::k_march<T, NT, false, false, PIPE>;
     k.stage[2] = fused::k_march<T, NT, false, true, PIPE>;
+    k.dump = fused::k_march<T, NT, true, false, PIPE, true>;
     k.step_dt = fused::k_step_dt<T, NT>;
     k.smem = fused::march_smem_bytes<T, NT, PIPE>();
     k.nt = NT;
@@ -438,6 +442,7 @@ template <class T> class FusedEngine : public Engine {
     explicit FusedEngine(SolverCore* core) : core_(core) {}
     ~FusedEngine() override {
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (rdump_) cudaFree(rdump_);
         if (arena_) cudaFree(arena_);
         if (h_state_) cudaFreeHost(h_state_);
     }
@@ -447,9 +452,9 @@ template <class T> class FusedEngine : public Engine {
             err = "unsupported tile shape " + std::to_string(ti) + "x" + std::to_string(tj) + "x" + std::to_string(nt);
             return false;
         }
-        for (int k = 0; k < 3; ++k)
-            if (cudaFuncSetAttribute(K_.stage[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K_.smem) !=
-                cudaSuccess) {
+        for (int k = 0; k < 4; ++k)
+            if (cudaFuncSetAttribute(k < 3 ? K_.stage[k] : K_.dump, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)K_.smem) != cudaSuccess) {
                 err = "stage kernel needs " + std::to_string(K_.smem) + " bytes of shared memory";
                 return false;
             }
@@ -806,6 +811,25 @@ template <class T> class FusedEngine : public Engine {
         return JST_OK;
     }
 
+    // R = Fc - Fv - Fd - S of every cell of the current state from the stage
+    // kernel the RK stages run with (its DUMP instantiation of stage 0), after
+    // the time step of the current state, as the first stage of a step sees it.
+    jst_status stage_residual(double* out) override {
+        SolverCore& C = *core_;
+        size_t n = (size_t)C.ni * C.nj;
+        if (!rdump_) {
+            if (cudaMalloc(&rdump_, 5 * n * sizeof(double)) != cudaSuccess) return JST_ERR_OOM;
+            inst_.rdump = rdump_;
+            cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
+        }
+        launch_step_dt();
+        JST_LAUNCH(K_.dump, sgrid(), K_.nt, K_.smem, C.st, d_tiles_, d_ntiles_, d_inst_, 0, RK_ALPHA[0]);
+        if (cudaMemcpyAsync(out, rdump_, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, C.st) != cudaSuccess ||
+            cudaStreamSynchronize(C.st) != cudaSuccess)
+            return JST_ERR_CUDA;
+        return JST_OK;
+    }
+
     jst_status timestep(double* dt) override {
         launch_step_dt();
         InstState s;
@@ -954,6 +978,7 @@ template <class T> class FusedEngine : public Engine {
     bool tune_ = false;
     void* arena_ = nullptr;
     double* extra_hist_ = nullptr;
+    double* rdump_ = nullptr;
     size_t hist_cap_ = 0;
     Inst<T> inst_{};
     Inst<T>* d_inst_ = nullptr;
@@ -1597,7 +1622,7 @@ struct jst_batch {
     std::unique_ptr<jst::BatchBase> impl;
 };
 
-// Test hook (not in the public header): the marching kernels' FP64
+// Test hook (declared in include/jst_gpu_debug.h): the marching kernels' FP64
 // quotient, square root, exponential and inverse sixth root (jst::dv, sq, ex
 // with Q = true, and jst::rroot6) beside the library's, for n operand pairs:
 // out[8k..8k+7] = quick a/b, a/b, quick sqrt(b), sqrt(b), quick exp(a),

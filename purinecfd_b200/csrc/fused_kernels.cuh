@@ -86,6 +86,9 @@ template <class T> struct Inst {
     // {tau nx, ny of face row k; n nx, ny, 1/V, 1/d^2, V of cell row k-1; 0}
     // in the stage type (zeros for cell row -1), see k_march_geom
     const T* mg;
+    // residual dump (jst_stage_residual): 5 planes of NI*NJ doubles that the
+    // DUMP instantiation of stage 0 writes R = Fc - Fv - Fd - S into
+    double* rdump;
 };
 
 struct TileRef {
@@ -331,7 +334,10 @@ JST_D void async_wait_all() {
 
 // The stage kernel.  FIRST: stage 0 (reads U_n, adds dt to the total time).
 // LAST: stage 4 (writes U_n in place, residual, next step's time step).
-template <class T, int TI, int TJ, int NT, bool FIRST, bool LAST>
+// DUMP (with FIRST only): the residual R of every cell of the current state
+// goes to Inst::rdump instead of an update; nothing else is written and the
+// instance's step counters and stop flags are ignored.
+template <class T, int TI, int TJ, int NT, bool FIRST, bool LAST, bool DUMP = false>
 __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles, const Inst<T>* insts, int stage,
                                               double alpha) {
     using L = Layout<T, TI, TJ, NT>;
@@ -362,12 +368,12 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
         int step = st->step;
         unsigned long long stage_id = (unsigned long long)step * 5 + stage;
         unsigned long long bad = st->bad;
-        int skip = st->done || step >= st->max_step || (bad != NO_BAD && (bad >> 32) < stage_id);
+        int skip = !DUMP && (st->done || step >= st->max_step || (bad != NO_BAD && (bad >> 32) < stage_id));
         flags[0] = skip;
         flags[1] = FIRST ? st->fresh : 0;
         flags[2] = step;
         adt_s = alpha * st->dt;  // the step's global time step, read once per tile
-        if (FIRST && !skip && tr.tile == 0) st->totaltime += st->dt;
+        if (FIRST && !DUMP && !skip && tr.tile == 0) st->totaltime += st->dt;
     }
     JST_SYNC();
     if (flags[0]) {
@@ -462,7 +468,7 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
     }
     async_wait_all();
     // primitives of the interior rows; periodic ghost columns are re-packed
-    // from their primitives (boundary.rs:54-72, state.rs:490-505)
+    // from their primitives (boundary.rs:54-72, state.rs:143-156)
 #pragma unroll
     for (int q = 0; q < KA; ++q) {
         int w = tid + q * NT;
@@ -709,6 +715,10 @@ __global__ void __launch_bounds__(NT) k_stage(const TileRef* tiles, int* ntiles,
         for (int k = 0; k < 5; ++k)
             R[k] = (sFt[k * L::NFT + w + TJ] - sFt[k * L::NFT + w]) + (sFn[k * L::NFN + fd + 1] - sFn[k * L::NFN + fd]);
         R[4] -= sS[w];
+        if constexpr (DUMP) {
+            for (int k = 0; k < 5; ++k) I.rdump[k * (long)ni * nj + id] = (double)R[k];
+            continue;
+        }
         int rc = (ti + 1) * RJ + tj + 1;  // ring index of the cell
         double a = I.local_dt ? alpha * ld(I.ldt + id) : adt_s;
         double sc = a * gs[L::gIV + rc];

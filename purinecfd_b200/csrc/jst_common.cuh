@@ -25,7 +25,7 @@
 
 namespace jst {
 
-// Per-solve constants: config.rs:88-189 inputs and config.rs:191-223 derived
+// Per-solve constants: config.rs:11-111 inputs and config.rs:115-145, 173-206 derived
 // values, plus a few constant sub-expressions the reference evaluates inline
 // (each is a pure function of constants, so precomputing it is exact).
 struct PhysConst {
@@ -44,7 +44,7 @@ struct PhysConst {
     double fw_lim;       // (1 + Cw3^6)^(1/6), the limit of fw for large g
     int supersonic;
     int halo;
-    // Free-stream primitive state written by Cells::initialize (state.rs:522-539).
+    // Free-stream primitive state written by Cells::initialize (state.rs:174-190).
     double f_rho, f_p, f_t, f_vx, f_vy, f_e, f_h, f_c, f_nut, f_mu;
 };
 
@@ -178,7 +178,7 @@ template <class T, bool Q = false> JST_HD Prim<T> unpack_cell(T u0, T u1, T u2, 
     return q;
 }
 
-// Cells::pack (state.rs:490-505).
+// Cells::pack (state.rs:143-156).
 template <class T> JST_HD void pack_cell(const Prim<T>& q, T* u) {
     u[0] = q.rho;
     u[1] = q.rho * q.vx;
@@ -187,7 +187,7 @@ template <class T> JST_HD void pack_cell(const Prim<T>& q, T* u) {
     u[4] = q.rho * q.nut;
 }
 
-// Config::mu, Sutherland (config.rs:287-291).
+// Config::mu, Sutherland (config.rs:210-213).
 template <class T, bool Q = false> JST_HD T mu_of(T t, T inv_t_ref, T suth_num, T t_suth) {
     T r = t * inv_t_ref;
     return dv<T, Q>(r * sq<T, Q>(r) * suth_num, t + t_suth);

@@ -229,7 +229,10 @@ template <class T, int NT> constexpr int march_min_blocks() {
 // PIPE: every global input of row k+1 is copied into a per-warp shared
 // buffer (cp.async) while row k is computed, so the walk never waits on HBM
 // latency; without PIPE the loads are issued in the row that uses them.
-template <class T, int NT, bool FIRST, bool LAST, bool PIPE = false>
+// DUMP (with FIRST only): the residual R of every cell of the current state
+// goes to Inst::rdump instead of an update; nothing else is written and the
+// instance's step counters and stop flags are ignored.
+template <class T, int NT, bool FIRST, bool LAST, bool PIPE = false, bool DUMP = false>
 __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage,
                                               double alpha) {
     using TD = typename std::conditional<LAST, double, T>::type;
@@ -275,10 +278,10 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             int step = st->step;
             unsigned long long sid = (unsigned long long)step * 5 + stage;
             unsigned long long bad = st->bad;
-            hdr[0] = st->done || step >= st->max_step || (bad != NO_BAD && (bad >> 32) < sid);
+            hdr[0] = !DUMP && (st->done || step >= st->max_step || (bad != NO_BAD && (bad >> 32) < sid));
             hdr[1] = FIRST ? st->fresh : 0;
             hdr[2] = step;
-            if (FIRST && !hdr[0] && tr.tile == 0) st->totaltime += st->dt;
+            if (FIRST && !DUMP && !hdr[0] && tr.tile == 0) st->totaltime += st->dt;
         }
         const int skip = jst_shfl_idx(hdr[0], 0);
         if (skip) continue;
@@ -626,7 +629,16 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 // the inputs of all 32 lanes, wrapped columns for the halo
                 // lanes) and only the output lanes store, so the update is one
                 // straight block; without it only the output lanes load.
-                if (PIPE || out_lane) {
+                if constexpr (DUMP) {
+                    if (out_lane) {
+                        const long id = (long)m * nj + gj;
+                        for (int v = 0; v < 5; ++v) {
+                            T Rv = (ftn[v] - ft[v]) + (fnr[v] - fn[v]);
+                            if (v == 4) Rv -= sw[0];
+                            I.rdump[v * np + id] = (double)Rv;
+                        }
+                    }
+                } else if (PIPE || out_lane) {
                     const long id = (long)m * nj + gj;
                     T R[5];
                     for (int v = 0; v < 5; ++v) R[v] = (ftn[v] - ft[v]) + (fnr[v] - fn[v]);

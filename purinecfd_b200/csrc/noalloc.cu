@@ -10,6 +10,7 @@
 // so this entry point takes device pointers for all three and keeps its only
 // scratch — one partial sum per thread block — in a fixed file-scope
 // __device__ array.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -33,10 +34,46 @@ constexpr long kMaxCells = (long)kMaxBlocks * kCellsPerBlock;  // 16,777,216 cel
 // library holds it until the process exits.  All calls share it.
 static __device__ __align__(256) double g_noalloc_partials[kMaxBlocks];
 
-// Device addresses of g_noalloc_partials, one per device, looked up once.
+// Device addresses of g_noalloc_partials, one per device, looked up once per
+// CUDA context: each entry remembers the unique id (cuCtxGetId) of the
+// context it was looked up in, so a context created later on the same device
+// (after cudaDeviceReset, or a driver context made current by the host) gets
+// its own lookup instead of a stale address.
 constexpr int kMaxDevices = 64;
-double* g_partials_addr[kMaxDevices] = {};
+struct ScratchAddr {
+    unsigned long long ctx_id;
+    double* ptr;
+};
+ScratchAddr g_partials_addr[kMaxDevices] = {};
 std::mutex g_partials_mu;
+
+// cuCtxGetCurrent and cuCtxGetId through the runtime's driver entry points
+// (the library does not link libcuda itself).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+bool current_context_id(unsigned long long* id, std::string* err) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa{}, qb{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess || !a || !b) {
+            *err = "cuCtxGetCurrent / cuCtxGetId not available from the CUDA driver";
+            return false;
+        }
+        get_current = reinterpret_cast<CtxGetCurrentFn>(a);
+        get_id = reinterpret_cast<CtxGetIdFn>(b);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS) {
+        *err = "no current CUDA context for the residual scratch lookup";
+        return false;
+    }
+    return true;
+}
 
 // Fixed-shape per-block sums: thread t adds cells t, t+256, ... of the block's
 // chunk in order, then a tree over the 256 threads.  Deterministic.
@@ -78,7 +115,8 @@ __global__ void __launch_bounds__(kThreads) k_noalloc_final(const double* partia
     if (threadIdx.x == 0) *out = sqrt(red[0] / (double)ni / (double)nj);
 }
 
-// Device address of the scratch on the current device (set-up on first use).
+// Device address of the scratch on the current device (set-up on the first
+// call in each context, with that device current).
 double* partials_on_current_device(std::string* err) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -90,17 +128,26 @@ double* partials_on_current_device(std::string* err) {
         *err = "device ordinal out of range for the residual scratch table";
         return nullptr;
     }
+    // The entry is valid while the context it was looked up in is the
+    // current one.  A thread with no current context yet gets one from the
+    // lookup itself (cudaGetSymbolAddress makes the device's primary context
+    // current), so the id is read again after it.
+    unsigned long long ctx = 0;
+    std::string no_ctx;
+    const bool have_ctx = current_context_id(&ctx, &no_ctx);
     std::lock_guard<std::mutex> lock(g_partials_mu);
-    if (!g_partials_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-        if (e != cudaSuccess || !p) {
-            *err = std::string("cudaGetSymbolAddress failed for the residual scratch: ") + cudaGetErrorString(e);
-            return nullptr;
-        }
-        g_partials_addr[dev] = static_cast<double*>(p);
+    ScratchAddr& slot = g_partials_addr[dev];
+    if (have_ctx && slot.ptr && slot.ctx_id == ctx) return slot.ptr;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess || !p) {
+        *err = std::string("cudaGetSymbolAddress failed for the residual scratch: ") + cudaGetErrorString(e);
+        return nullptr;
     }
-    return g_partials_addr[dev];
+    if (!current_context_id(&ctx, err)) return nullptr;
+    slot.ptr = static_cast<double*>(p);
+    slot.ctx_id = ctx;
+    return slot.ptr;
 }
 
 }  // namespace

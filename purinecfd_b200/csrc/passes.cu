@@ -171,7 +171,7 @@ __device__ __forceinline__ void pack_at(const PS& s, long i, long j) {
     s.U[4](i, j) = r * s.nut(i, j);
 }
 
-// Cells::initialize (state.rs:522-539) for interior cells.
+// Cells::initialize (state.rs:174-190) for interior cells.
 __global__ void k_init(PS s, PhysConst c) {
     long id = gtid();
     if (id >= (long)s.ni * s.nj) return;
@@ -191,7 +191,7 @@ __global__ void k_init(PS s, PhysConst c) {
     s.fv1(i, j) = 0.0;
 }
 
-// state.rs:547-552 for every addressable cell.
+// state.rs:198-203 for every addressable cell.
 __global__ void k_set_uniform(PS s, double rho, double p, double t, double vx, double vy, double e, double h,
                               double cc, double nut) {
     long W = s.nj + 2 * s.H;
@@ -782,7 +782,7 @@ void passes_init(Passes* P, const Geom& g, const PhysConst& c, cudaStream_t st) 
 
 void passes_set_uniform(Passes* P, const PhysConst& c, double rho, double vx, double vy, double p, double nut,
                         cudaStream_t st) {
-    // PrimState::from_primitives (state.rs:569-587)
+    // PrimState::from_primitives (state.rs:222-237)
     double t = p / (c.r_gas * rho);
     double e = p / (rho * c.gm1) + 0.5 * (vx * vx + vy * vy);
     double h = e + p / rho;

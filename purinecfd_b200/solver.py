@@ -43,7 +43,9 @@ EXPORTS = ["jst_default_opts", "jst_create_from_paths", "jst_create", "jst_destr
            "jst_nj", "jst_advance", "jst_run", "jst_residual_terms", "jst_timestep", "jst_residual",
            "jst_totaltime", "jst_step_count", "jst_get_field", "jst_get_faces", "jst_set_conserved",
            "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps", "jst_residual_noalloc", "jst_kernel_config",
-           "jst_checkpoint_save", "jst_checkpoint_load"]
+           "jst_checkpoint_save", "jst_checkpoint_load", "jst_stage_residual"]
+# test hooks declared in include/jst_gpu_debug.h
+DEBUG_EXPORTS = ["jst_debug_set_uniform", "jst_debug_kernel", "jst_debug_quick_arith"]
 
 
 class Opts(C.Structure):
@@ -71,7 +73,7 @@ class JstError(RuntimeError):
 
 
 class NonPhysical(JstError):
-    """state.rs:589-606: raised instead of producing NaNs."""
+    """state.rs:242-257: raised instead of producing NaNs."""
 
     def __init__(self, i, j, rho, p):
         self.i, self.j, self.rho, self.p = i, j, rho, p
@@ -109,6 +111,7 @@ def lib() -> C.CDLL:
         L.jst_advance.argtypes = [vp, C.POINTER(NonPhysicalC)]
         L.jst_run.argtypes = [vp, C.c_int64, STEP_CB, vp, C.POINTER(RunReportC), C.POINTER(NonPhysicalC)]
         L.jst_residual_terms.argtypes = [vp, pd]
+        L.jst_stage_residual.argtypes = [vp, pd, sz]
         L.jst_timestep.argtypes = [vp, pd]
         L.jst_residual.argtypes = [vp, pd]
         L.jst_totaltime.argtypes = [vp, pd]
@@ -227,6 +230,15 @@ class Solver:
         dt = C.c_double(0.0)
         self._check(lib().jst_residual_terms(self._h, C.byref(dt) if with_timestep else None))
         return dt.value if with_timestep else None
+
+    def stage_residual(self) -> np.ndarray:
+        """R = Fc - Fv - Fd (R[4] -= S) of every cell of the current state, as
+        the RK update applies it (solver.rs:128-133), from the stage kernel this
+        solver runs with; shape (5, NI, NJ)."""
+        n = self.ni * self.nj
+        out = np.empty(5 * n)
+        self._check(lib().jst_stage_residual(self._h, _ptr(out), out.size))
+        return out.reshape(5, self.ni, self.nj)
 
     def timestep(self) -> float:
         """timestep::compute (timestep.rs:24-57)."""

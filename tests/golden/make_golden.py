@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Regenerate the golden fixtures in this directory from the reference.
 
-Run in a container where the reference is mounted (default /root/reference);
-nothing at test time reads the reference, only the files written here.
+Run where a checkout of the reference is available and pass its root
+directory with --reference; nothing at test time reads the reference, only
+the files written here.
 
 What it writes:
 
@@ -23,7 +24,7 @@ What it writes:
   so that v_inf != 0 and a different Mach number are pinned too.  Its mesh is
   written as ``ell_13x40.txt``.
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py --reference <root of the reference checkout>
 """
 
 from __future__ import annotations
@@ -76,7 +77,7 @@ def max_dev(a: dict, b: dict) -> float:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root directory of the reference checkout")
     args = ap.parse_args()
     ref = Path(args.reference)
     jstpy = ref / "jst-py"

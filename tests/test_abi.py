@@ -38,8 +38,24 @@ def test_python_binding_lists_every_export():
     (the solver module or the batch module), and nothing else is listed."""
     from purinecfd_b200 import batch, solver
     declared = set(declared_functions())
-    bound = set(solver.EXPORTS) | set(batch.BATCH_EXPORTS)
+    bound = set(solver.EXPORTS) | set(solver.DEBUG_EXPORTS) | set(batch.BATCH_EXPORTS)
     assert declared == bound, (sorted(declared - bound), sorted(bound - declared))
+
+
+def test_library_exports_nothing_undeclared():
+    """Every jst_* symbol the library exports is declared in include/*.h (the
+    public ABI in jst_gpu.h, the test hooks in jst_gpu_debug.h)."""
+    import shutil
+    import subprocess
+    from purinecfd_b200 import solver
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not available")
+    out = subprocess.run([nm, "-D", "--defined-only", str(solver.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if ln.split() and ln.split()[-1].startswith("jst_")}
+    undeclared = sorted(exported - set(declared_functions()))
+    assert not undeclared, undeclared
 
 
 def test_version_string():
