@@ -202,26 +202,58 @@ def replica_value(cells: int, steps: int, ms_max: float, world: int) -> float:
     return world * cells * 5 * steps / (ms_max / 1e3) / 1e6
 
 
-def cpu_reference(workload: str, timed_steps: int, warm_steps: int):
-    """Oracle (CPU restatement of jst-rs, FP64) on the host cores."""
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.lower().startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def thread_counts(nproc: int) -> list[int]:
+    """1, 2, 4, ... up to nproc, and nproc itself (the sweep of bin/jst.rs:43-48)."""
+    out, t = [], 1
+    while t < nproc:
+        out.append(t)
+        t *= 2
+    return out + [nproc]
+
+
+def cpu_reference(workload: str, timed_steps: int, warm_steps: int, sweep: list[int] | None = None):
+    """Oracle (CPU restatement of jst-rs, FP64) on the host cores.  With a
+    sweep, one RK step is timed at each thread count and the timed steps run
+    at the fastest one; the result reports every point."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import jst_oracle as jo
     from purinecfd_b200 import workloads
     cfg, xy, nr, nt = workloads.WORKLOADS[workload]()
-    cores = os.cpu_count() or 1
-    jo.set_threads(cores)
+    nproc = os.cpu_count() or 1
+    jo.set_threads(nproc)
     t0 = time.perf_counter()
     o = jo.OracleSolver(cfg, xy, nr, nt)
     t_setup = time.perf_counter() - t0
+    cells = o.n_cells
     if warm_steps:
         o.run(warm_steps)
+    points = {}
+    best = nproc
+    if sweep:
+        for t in sweep:
+            jo.set_threads(t)
+            t0 = time.perf_counter()
+            o.run(1)
+            points[t] = cells * 5 / (time.perf_counter() - t0) / 1e6
+        best = max(points, key=points.get)
+    jo.set_threads(best)
     t0 = time.perf_counter()
     o.run(timed_steps)
     dt = time.perf_counter() - t0
-    cells = o.n_cells
     o.close()
-    return {"value": cells * 5 * timed_steps / dt / 1e6, "cores": cores, "seconds": dt, "setup_s": t_setup,
-            "steps": timed_steps, "cells": cells}
+    return {"value": cells * 5 * timed_steps / dt / 1e6, "cores": best, "nproc": nproc, "seconds": dt,
+            "setup_s": t_setup, "steps": timed_steps, "cells": cells, "cpu": cpu_model(),
+            "sweep": {str(k): round(v, 3) for k, v in points.items()}}
 
 
 def run_reference(args, world, rank):
@@ -229,16 +261,18 @@ def run_reference(args, world, rank):
         return
     steps = max(1, min(args.steps, 3))
     warm = 1 if args.warmup > 0 else 0
-    r = cpu_reference(args.workload, steps, warm)
+    nproc = os.cpu_count() or 1
+    r = cpu_reference(args.workload, steps, warm, sweep=sorted({max(1, nproc // 2), nproc}))
     sample = (f"{args.workload}: {r['cells']} cells, {warm} untimed + {steps} timed RK steps of the oracle "
-              f"(CPU FP64 restatement of jst-rs; Rust toolchain absent), {r['cores']} OpenMP threads")
+              f"(CPU FP64 restatement of jst-rs; Rust toolchain absent), {r['cores']} OpenMP threads "
+              f"(best of {sorted(int(k) for k in r['sweep'])} of {r['nproc']}), {r['cpu']}")
     line = {"metric": METRIC, "value": round(r["value"], 3), "unit": UNIT, "n_gpus": 0, "steps": steps,
             "warmup": warm, "ms_per_step": round(1e3 * r["seconds"] / steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": args.workload, "precision": "fp64", "path": "cpu oracle"},
             "cpu_baseline": {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "cpu": r["cpu"], "nproc": r["nproc"], "sweep": r["sweep"]},
             "e2e": {"value": round(r["value"], 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -329,17 +363,25 @@ def run_ours(args, world, rank, local):
                            "seconds": round(t_e2e, 4),
                            "what": "jst_create from host nodes + jst_run with per-step residual callback + "
                                    "6 fields read back"}
-    # every rank takes part in the batch leg (its instances are dealt over the ranks)
+    # every rank takes part in the batch and serving legs (instances are dealt over the ranks)
     if args.batch_instances > 0:
         batch = batched_leg(args, world, rank)
         if rank == 0:
             line["batch"] = batch
+    if args.serve_requests > 0 and not args.no_serve:
+        sv = serve_leg(args, world, rank, rates=[float(x) for x in args.serve_line_rates.split(",")])
+        if rank == 0:
+            line["serve"] = sv
     if rank == 0:
         if world == 1 and not args.no_cpu:
-            r = cpu_reference(args.workload, 2, 1)
-            line["cpu_baseline"] = {"value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
-                                    "sample": f"{args.workload}: {r['cells']} cells, 1 untimed + 2 timed RK steps, "
-                                              f"oracle (CPU FP64 restatement of jst-rs), {r['cores']} threads"}
+            r = cpu_reference(args.workload, 2, 1, sweep=thread_counts(os.cpu_count() or 1))
+            line["cpu_baseline"] = {
+                "value": round(r["value"], 3), "unit": UNIT, "cores": r["cores"], "kind": "port",
+                "sample": f"{args.workload}: {r['cells']} cells, oracle (CPU FP64 restatement of jst-rs; Rust "
+                          f"toolchain absent); 1 untimed step, then one step at each thread count of the sweep, "
+                          f"then 2 timed RK steps at the fastest count ({r['cores']} of {r['nproc']})",
+                "cpu": r["cpu"], "nproc": r["nproc"], "sweep_mcell_stage_per_s": r["sweep"],
+                "ns_per_cell_step": round(1e9 * r["seconds"] / (r["cells"] * r["steps"]), 2)}
         print(json.dumps(line), flush=True)
 
 
@@ -363,130 +405,135 @@ def split_vs_fp64(cfg, xy, nr, nt, device, steps: int = 100) -> dict:
     return {"steps": steps, "field_err_rel_scale": err, "cl_fp64": clb, "dcl": abs(cla - clb), "dcd": abs(cda - cdb)}
 
 
+BATCH_SEED = 20261203
+
+
+def stratified_sample(classes: list, m: int) -> list[int]:
+    """Indices of about m instances with the mesh-class mix of the whole list
+    (per class a share proportional to its count, at least one, the first
+    ones drawn)."""
+    by = {}
+    for k, c in enumerate(classes):
+        by.setdefault(c, []).append(k)
+    out = []
+    for c, ks in sorted(by.items()):
+        take = max(1, round(m * len(ks) / len(classes)))
+        out += ks[:take]
+    return sorted(out)
+
+
 def batched_leg(args, world: int = 1, rank: int = 0):
     """Config-4 distribution: NACA 4-digit instances on three mesh classes with
     seeded M, alpha, Re (local time stepping, CFL 1.0), solved (a) all at once
-    in one FP32-split batch, (b) all at once in FP64 as the CL/CD reference and
-    (c) a subsample one at a time in FP64 (batch of one).  Each instance
-    retires on a 1e-6 residual drop or at the step cap.  With several ranks the
-    instances are dealt round-robin (instance k on rank k mod N): they are
-    independent, so no data moves between GPUs; the job time is the slowest
-    rank's."""
+    in FP32-split batches, (b) all at once in FP64 batches as the CL/CD
+    reference and (c) a sample with the same mesh-class mix one at a time on
+    the plain FP64 path (a Solver per instance).  Every solve retires on a
+    1e-6 residual drop, on |CL(n) - CL(n-100)| < cl_tol, or at the step cap.
+    With several ranks the instances are dealt by purinecfd_b200.shard (least
+    work first); the job time is the slowest rank's."""
     from purinecfd_b200 import PREC_FP32_SPLIT, PREC_FP64, workloads
-    from purinecfd_b200.serve import batch_solve
-    cases = []
-    for k in range(rank, args.batch_instances, world):
-        cfg, xy, nr, nt, _ = workloads.batch_instance(20261203, k)
+    from purinecfd_b200.serve import solve_alone
+    from purinecfd_b200.shard import Group, solve_sharded
+    g = Group()
+    cases, classes = [], []
+    for k in range(args.batch_instances):
+        cfg, xy, nr, nt, _ = workloads.batch_instance(BATCH_SEED, k)
         cfg["simulation"]["CFL"] = 1.0
         cases.append((cfg, xy, nr, nt))
-    part = {"instances": len(cases), "cells": sum((c[2] - 1) * c[3] for c in cases)}
-    barrier(world)
+        classes.append(f"{nt + 1}x{nr}")
+    rules = dict(max_steps=args.batch_steps, residual_drop=1e-6, cl_tol=args.batch_cl_tol)
     kinfo = {}
-    split, part["wall_split"] = (batch_solve(cases, PREC_FP32_SPLIT, max_steps=args.batch_steps, info=kinfo)
-                                 if cases else ([], 0.0))
-    part["kernel"] = kinfo.get("kernel")
     barrier(world)
-    ref, part["wall_ref"] = batch_solve(cases, PREC_FP64, max_steps=args.batch_steps) if cases else ([], 0.0)
-    part["plain_m"], part["plain_wall"] = 0, 0.0
-    if rank == 0 and cases:
-        m = max(1, min(args.plain_instances, len(cases)))
-        _, part["plain_wall"] = batch_solve(cases[:m], PREC_FP64, max_instances=1, max_steps=args.batch_steps)
-        part["plain_m"] = m
-    dcl, dcd = [], []
-    for a, r in zip(split, ref):
-        if a.status != 8 and r.status != 8:
-            dcl.append(abs(a.cl - r.cl))
-            dcd.append(abs(a.cd - r.cd))
-    part.update(cell_steps=sum((r.ni * r.nj) * r.steps for r in split), steps=sum(r.steps for r in split),
-                converged=sum(1 for r in split if r.status == 0), nonphysical=sum(1 for r in split if r.status == 8),
-                within=sum(1 for x, y in zip(dcl, dcd) if x <= 1e-4 and y <= 1e-4),
-                dcl_max=max(dcl) if dcl else None, dcd_max=max(dcd) if dcd else None,
-                latencies=[r.t_done - r.t_submit for r in split])
-    parts = gather_objects(part, world)
-    return combine_batch_parts(parts, args.batch_steps) if rank == 0 else None
+    split, wall, _ = solve_sharded(cases, PREC_FP32_SPLIT, group=g, info=kinfo, steps_per_poll=50, **rules)
+    barrier(world)
+    ref, wall_ref, _ = solve_sharded(cases, PREC_FP64, group=g, steps_per_poll=50, **rules)
+    if rank != 0:
+        return None
+    n = len(cases)
+    cells = [(c[2] - 1) * c[3] for c in cases]
+    # plain FP64 one at a time on a sample with the batch's mesh-class mix;
+    # per class the mean solve time, weighted by the class counts of the batch
+    sample = stratified_sample(classes, args.plain_instances)
+    t_cls, n_cls, plain_cell_steps, plain_wall = {}, {}, 0, 0.0
+    for k in sample:
+        r = solve_alone(cases[k], PREC_FP64, poll=50, device=g.local_rank, **rules)
+        t_cls.setdefault(classes[k], []).append(r.t_done)
+        plain_cell_steps += cells[k] * r.steps
+        plain_wall += r.t_done
+    for c in classes:
+        n_cls[c] = n_cls.get(c, 0) + 1
+    plain_time_all = sum(n_cls[c] * float(np.mean(t_cls[c])) for c in n_cls)
+    plain_sps = n / plain_time_all
+    ok = [(a, r) for a, r in zip(split, ref) if a.status != 8 and r.status != 8]
+    dcl = [abs(a.cl - r.cl) for a, r in ok]
+    dcd = [abs(a.cd - r.cd) for a, r in ok]
+    conv = [k for k, a in enumerate(split) if a.status == 0]
+    bad_split = {k for k, a in enumerate(split) if a.status == 8}
+    bad_fp64 = {k for k, r in enumerate(ref) if r.status == 8}
+    cell_steps = sum(c * a.steps for c, a in zip(cells, split))
+    sps = n / wall
+    return {"instances": n, "ranks": world, "cells": sum(cells), "step_cap": args.batch_steps,
+            "rules": f"residual drop 1e-6, |dCL| < {args.batch_cl_tol:g} over 100 steps, cap {args.batch_steps}",
+            "kernel": kinfo.get("kernel"), "classes": {c: n_cls[c] for c in sorted(n_cls)},
+            "solves_per_s": round(sps, 3), "wall_s": round(wall, 3),
+            "mcell_stage_per_s": round(cell_steps * 5 / wall / 1e6, 1),
+            "converged": len(conv), "converged_solves_per_s": round(len(conv) / wall, 3),
+            "nonphysical": len(bad_split), "nonphysical_fp64": len(bad_fp64),
+            "nonphysical_in_both": len(bad_split & bad_fp64),
+            "mean_steps": round(sum(a.steps for a in split) / max(1, n), 1),
+            "fp64_batch_solves_per_s": round(n / wall_ref, 3) if wall_ref > 0 else None,
+            "fp64_batch_converged": sum(1 for r in ref if r.status == 0),
+            "plain_fp64_one_at_a_time": {
+                "sample": len(sample), "sample_classes": {c: len(v) for c, v in sorted(t_cls.items())},
+                "mean_s_per_class": {c: round(float(np.mean(v)), 4) for c, v in sorted(t_cls.items())},
+                "solves_per_s_matched": round(plain_sps, 3),
+                "mcell_stage_per_s": round(plain_cell_steps * 5 / plain_wall / 1e6, 1) if plain_wall else None,
+                "what": "a Solver per instance (autotuned stage kernel, CUDA graph per step), FP64, the same "
+                        "stopping rules checked every 50 steps; solves/s for the batch's class mix = instances / "
+                        "sum over classes of (count x mean solve time of the sampled instances of that class)"},
+            "speedup_vs_plain": round(sps / (plain_sps * world), 2),
+            "speedup_vs_plain_cell_steps": round((cell_steps * 5 / wall) / (plain_cell_steps * 5 / plain_wall), 2)
+            if plain_wall else None,
+            "cl_err_max": max(dcl) if dcl else None, "cd_err_max": max(dcd) if dcd else None,
+            "within_1e-4": f"{sum(1 for x, y in zip(dcl, dcd) if x <= 1e-4 and y <= 1e-4)}/{n}",
+            "what": f"seed {BATCH_SEED}, PCG64 stream per instance; local time step; CL/CD error of the split batch "
+                    "vs the FP64 batch on the same instances (instances not NonPhysical in either); "
+                    "instances dealt over the ranks by purinecfd_b200.shard, plain sample on rank 0 counted "
+                    "once per GPU"}
 
 
-def gather_objects(obj, world: int) -> list:
-    if world == 1:
-        return [obj]
-    import torch.distributed as dist
-    out = [None] * world
-    dist.all_gather_object(out, obj)
-    return out
-
-
-def combine_batch_parts(parts: list, step_cap: int) -> dict:
-    """Job-level batch figures from the per-rank parts."""
-    from purinecfd_b200.serve import percentile
-    world = len(parts)
-    n = sum(p["instances"] for p in parts)
-    wall = max(p["wall_split"] for p in parts)
-    wall_ref = max(p["wall_ref"] for p in parts)
-    lat = [x for p in parts for x in p["latencies"]]
-    p0 = parts[0]
-    plain_sps = p0["plain_m"] / p0["plain_wall"] if p0["plain_wall"] > 0 else None
-    errs = [p["dcl_max"] for p in parts if p["dcl_max"] is not None]
-    errd = [p["dcd_max"] for p in parts if p["dcd_max"] is not None]
-    out = {"instances": n, "ranks": world, "cells": sum(p["cells"] for p in parts), "step_cap": step_cap,
-           "kernel": parts[0].get("kernel"),
-           "solves_per_s": round(n / wall, 3) if wall > 0 else None, "wall_s": round(wall, 3),
-           "mcell_stage_per_s": round(sum(p["cell_steps"] for p in parts) * 5 / wall / 1e6, 1) if wall > 0 else None,
-           "p50_s": round(percentile(lat, 50), 3), "p99_s": round(percentile(lat, 99), 3),
-           "converged": sum(p["converged"] for p in parts), "nonphysical": sum(p["nonphysical"] for p in parts),
-           "mean_steps": round(sum(p["steps"] for p in parts) / max(1, n), 1),
-           "fp64_batch_solves_per_s": round(n / wall_ref, 3) if wall_ref > 0 else None,
-           "plain_fp64_one_at_a_time": {"instances": p0["plain_m"],
-                                        "solves_per_s_per_gpu": None if plain_sps is None else round(plain_sps, 3),
-                                        "solves_per_s_job": None if plain_sps is None else round(plain_sps * world, 3),
-                                        "wall_s": round(p0["plain_wall"], 3)},
-           "speedup_vs_plain": round((n / wall) / (plain_sps * world), 2) if plain_sps and wall > 0 else None,
-           "cl_err_max": max(errs) if errs else None, "cd_err_max": max(errd) if errd else None,
-           "within_1e-4": f"{sum(p['within'] for p in parts)}/{n}",
-           "what": "seed 20261203, PCG64 stream per instance; local time step; retire at residual drop 1e-6 "
-                   "or step cap; CL/CD error vs the FP64 batch on the same instances; instances dealt "
-                   "round-robin over the ranks, plain one-at-a-time measured on rank 0 and counted once per GPU"}
-    return out
-
-
-def serve_sweep(args, world: int = 1, rank: int = 0):
-    """Serving stream (config-5 draws) at each rate.  With several ranks the
-    request stream is dealt round-robin (request k to rank k mod N), which
-    splits the Poisson arrivals into N Poisson streams of rate R/N; each rank
-    serves its share on its own GPU and rank 0 prints the job figures."""
-    from purinecfd_b200.serve import request_stream, serve
+def serve_leg(args, world: int = 1, rank: int = 0, rates=None, plain: bool = True):
+    """Serving stream (config-5 draws: the batch distribution plus cylinders)
+    with Poisson arrivals at each rate: the continuous-batching server
+    (FP32-split) and, for comparison, the plain FP64 path serving the same
+    stream one request at a time.  Requests are dealt over the ranks by
+    purinecfd_b200.shard.  Returns the job figures (rank 0)."""
+    from purinecfd_b200 import PREC_FP64
+    from purinecfd_b200.serve import request_stream
+    from purinecfd_b200.shard import Group, serve_sharded
+    g = Group()
     out = []
-    for rate in [float(x) for x in args.serve_rates.split(",")]:
-        reqs = request_stream(20261203, args.serve_requests, max_steps=args.batch_steps)[rank::world]
-        barrier(world)
-        st, results = serve(reqs, rate / world, seed=int(rate) * world + rank) if reqs else (None, [])
-        part = {"rate": rate, "requests": len(reqs), "completed": len(results),
-                "converged": sum(1 for x in results if x[1].status == 0),
-                "nonphysical": sum(1 for x in results if x[1].status == 8),
-                "wall_s": st.wall_s if st else 0.0, "latencies": [x[2] for x in results],
-                "steps": [x[1].steps for x in results]}
-        parts = gather_objects(part, world)
-        if rank == 0:
-            job = combine_serve_parts(parts)
-            out.append(job)
-            print(json.dumps({"serve": job}), flush=True)
-    return out
-
-
-def combine_serve_parts(parts: list) -> dict:
-    """Job-level serving figures from the per-rank parts: all requests count,
-    the job lasts as long as the slowest rank, latency percentiles over every
-    request."""
-    from purinecfd_b200.serve import percentile
-    wall = max(p["wall_s"] for p in parts)
-    lat = [x for p in parts for x in p["latencies"]]
-    steps = [x for p in parts for x in p["steps"]]
-    done = sum(p["completed"] for p in parts)
-    return {"rate": parts[0]["rate"], "ranks": len(parts), "requests": sum(p["requests"] for p in parts),
-            "completed": done, "converged": sum(p["converged"] for p in parts),
-            "nonphysical": sum(p["nonphysical"] for p in parts), "wall_s": wall,
-            "solves_per_s": done / wall if wall > 0 else None,
-            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99),
-            "mean_steps": sum(steps) / len(steps) if steps else None}
+    for rate in rates or [float(x) for x in args.serve_rates.split(",")]:
+        reqs = request_stream(BATCH_SEED, args.serve_requests, max_steps=args.batch_steps)
+        row = {"rate": rate}
+        legs = [("batched_split", {})]
+        if plain:
+            legs.append(("plain_fp64", dict(precision=PREC_FP64, max_instances=1)))
+        for name, kw in legs:
+            barrier(world)
+            st, _ = serve_sharded(reqs, rate, seed=int(rate), group=g, **kw)
+            row[name] = {"completed": st.completed, "converged": st.converged, "nonphysical": st.nonphysical,
+                         "wall_s": round(st.wall_s, 3), "solves_per_s": round(st.solves_per_s, 3),
+                         "p50_s": round(st.p50_s, 4), "p99_s": round(st.p99_s, 4),
+                         "mean_steps": round(st.mean_steps, 1)}
+        if plain and row["plain_fp64"]["solves_per_s"]:
+            row["speedup_solves_per_s"] = round(row["batched_split"]["solves_per_s"] /
+                                                row["plain_fp64"]["solves_per_s"], 2)
+        out.append(row)
+        if rank == 0 and args.serve:
+            print(json.dumps({"serve": row}), flush=True)
+    return {"requests": args.serve_requests, "ranks": world, "step_cap": args.batch_steps,
+            "rules": "residual drop 1e-6 or |dCL| < 1e-5 over 100 steps", "rates": out} if rank == 0 else None
 
 
 def main():
@@ -502,11 +549,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--batch-instances", type=int, default=256, help="config-4 batch size (0 = skip)")
-    ap.add_argument("--batch-steps", type=int, default=1000, help="step cap per batched instance")
-    ap.add_argument("--plain-instances", type=int, default=32, help="FP64 one-at-a-time subsample")
+    ap.add_argument("--batch-steps", type=int, default=2000, help="step cap per batched instance")
+    ap.add_argument("--batch-cl-tol", type=float, default=1e-5, help="CL window tolerance of the batch leg")
+    ap.add_argument("--plain-instances", type=int, default=24, help="FP64 one-at-a-time sample (class mix kept)")
     ap.add_argument("--serve", action="store_true", help="run the serving sweep instead of the benchmark")
-    ap.add_argument("--serve-rates", default="1,10,50,200")
-    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-rates", default="1,10,50,200", help="rates of the --serve sweep")
+    ap.add_argument("--serve-line-rates", default="10,200", help="rates of the serving summary in the line")
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving summary")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -514,7 +564,7 @@ def main():
                                                                    int(os.environ.get("RANK", "0")), 0)
     try:
         if args.serve:
-            serve_sweep(args, world, rank)
+            serve_leg(args, world, rank)
             return
         if args.impl == "reference":
             run_reference(args, world, rank)

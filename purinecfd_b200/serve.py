@@ -69,15 +69,25 @@ class ServeStats:
     mean_steps: float
 
 
+def poisson_arrivals(n: int, rate: float, seed: int = 0) -> np.ndarray:
+    """Arrival offsets (seconds, the first at 0) of n requests of a Poisson
+    stream at `rate` requests/s."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=n)
+    return np.cumsum(gaps) - gaps[0] if n else gaps
+
+
 def serve(requests: list[Request], rate: float, seed: int = 0, precision: int = PREC_FP32_SPLIT,
           hbm_budget_gb: float = 150.0, max_instances: int = 512, steps_per_poll: int = 25,
-          chunk: int = 25) -> tuple[ServeStats, list]:
-    """Run the request list with Poisson arrivals at `rate` requests/s (real time)."""
-    rng = np.random.default_rng(seed)
-    gaps = rng.exponential(1.0 / rate, size=len(requests))
-    arrivals = np.cumsum(gaps) - gaps[0]
+          chunk: int = 25, arrivals: np.ndarray | None = None, device: int = 0) -> tuple[ServeStats, list]:
+    """Run the request list with Poisson arrivals at `rate` requests/s (real
+    time), or at the given arrival offsets (seconds from the start).  Returns
+    (statistics, [(request index, result, latency)] in completion order)."""
+    if arrivals is None:
+        arrivals = poisson_arrivals(len(requests), rate, seed)
+    arrivals = np.asarray(arrivals, dtype=float)
     b = Batch(precision=precision, dt_mode=DT_LOCAL, steps_per_poll=steps_per_poll, hbm_budget_gb=hbm_budget_gb,
-              max_instances=max_instances)
+              max_instances=max_instances, device=device)
     t0 = time.perf_counter()
     arrival_of = {}
     nxt = 0
@@ -111,12 +121,13 @@ def serve(requests: list[Request], rate: float, seed: int = 0, precision: int = 
 
 
 def batch_solve(cases, precision: int, max_instances: int = 256, max_steps: int = 2000, residual_drop: float = 1e-6,
-                cl_tol: float = 0.0, hbm_budget_gb: float = 40.0, steps_per_poll: int = 25, info: dict | None = None):
+                cl_tol: float = 0.0, hbm_budget_gb: float = 40.0, steps_per_poll: int = 25, info: dict | None = None,
+                device: int = 0):
     """Solve every case (config, xy, n_rings, n_theta) in one batch; returns
     (results in case order, wall seconds).  `info`, when given, receives the
     stage kernel configuration the batch ran with."""
     b = Batch(precision=precision, dt_mode=DT_LOCAL, steps_per_poll=steps_per_poll, hbm_budget_gb=hbm_budget_gb,
-              max_instances=max_instances)
+              max_instances=max_instances, device=device)
     t0 = time.perf_counter()
     ids = [b.submit(c[0], c[1], c[2], c[3], max_steps, residual_drop, cl_tol) for c in cases]
     res = {r.id: r for r in b.run_all(chunk=max(steps_per_poll, 100))}
@@ -125,6 +136,50 @@ def batch_solve(cases, precision: int, max_instances: int = 256, max_steps: int 
         info["kernel"] = "x".join(map(str, b.kernel_config()))
     b.close()
     return [res[i] for i in ids], wall
+
+
+def solve_alone(case, precision: int, max_steps: int = 2000, residual_drop: float = 1e-6, cl_tol: float = 0.0,
+                poll: int = 50, device: int = 0):
+    """One solve on its own (the plain one-at-a-time path: a Solver with its
+    autotuned stage kernel and a CUDA graph per RK step, local time steps)
+    under the batch's stopping rules, checked every `poll` steps: residual
+    below residual_drop times the first step's residual, |CL(n) - CL(n-100)|
+    below cl_tol (CL sampled every `poll` steps), or the step limit.  Returns
+    a BatchResult (status JST_OK converged, JST_ERR_NONPHYSICAL, or
+    JST_ERR_TIMEOUT at the limit)."""
+    from .batch import BatchResult
+    from .solver import NonPhysical, Solver
+    cfg, xy, nr, nt = case
+    t0 = time.perf_counter()
+    s = Solver(cfg, xy, nr, nt, precision=precision, dt_mode=DT_LOCAL, device=device)
+    status, steps, first, res = 10, 0, float("nan"), float("nan")
+    cl_hist = []
+    cl = cd = float("nan")
+    try:
+        s.run(1)
+        steps, first = 1, s.residual()
+        res = first
+        while steps < max_steps:
+            n = min(poll - steps % poll, max_steps - steps)
+            rep = s.run(n)
+            steps += rep.steps
+            res = rep.residual
+            if residual_drop > 0 and res < residual_drop * first:
+                status = 0
+                break
+            if cl_tol > 0 and steps % poll == 0:
+                cl_hist.append((steps, s.forces()[0]))
+                old = [c for k, c in cl_hist if steps - k >= 100]
+                if old and abs(cl_hist[-1][1] - old[-1]) < cl_tol:
+                    status = 0
+                    break
+        cl, cd = s.forces()
+    except NonPhysical:
+        status = 8
+    ni, nj = s.ni, s.nj
+    s.close()
+    t1 = time.perf_counter()
+    return BatchResult(-1, status, steps, res, first, float("nan"), cl, cd, 0.0, 0.0, t1 - t0, ni, nj)
 
 
 def percentile(xs, q):

@@ -27,23 +27,15 @@ def _rank(rank: int, world: int, port: int, q):
     sys.path.insert(0, str(ROOT))
     import bench
     import torch.distributed as dist
+    from purinecfd_b200.shard import Group
     w, r, _ = bench.dist_setup("gloo")
     bench.barrier(w)
     ms = 100.0 + 25.0 * r  # rank 1 is the slow one
     m = bench.max_over_ranks(ms, w)
     bench.barrier(w)
-    parts = bench.gather_objects(_part(r), w)
+    parts = Group().gather({"rank": r})
     q.put((r, w, m, bench.replica_value(1000, 10, m, w), parts))
     dist.destroy_process_group()
-
-
-def _part(rank: int) -> dict:
-    """A batch-leg part as one rank reports it (instances k = rank, rank + 2, ...)."""
-    return {"instances": 3 - rank, "cells": 1000 * (3 - rank), "wall_split": 2.0 + rank, "wall_ref": 5.0 - rank,
-            "plain_m": 2 if rank == 0 else 0, "plain_wall": 4.0 if rank == 0 else 0.0,
-            "cell_steps": 10_000 * (3 - rank), "steps": 30 - 10 * rank, "converged": 1, "nonphysical": rank,
-            "within": 3 - 2 * rank, "dcl_max": 1e-6 * (rank + 1), "dcd_max": None if rank else 2e-7,
-            "latencies": [1.0 + rank, 2.0 + rank]}
 
 
 def test_two_rank_barrier_and_max_over_ranks():
@@ -61,27 +53,7 @@ def test_two_rank_barrier_and_max_over_ranks():
     for r, w, m, v, parts in out:
         assert w == 2 and m == 125.0
         assert v == pytest.approx(2 * 1000 * 5 * 10 / 0.125 / 1e6)
-        assert parts == [_part(0), _part(1)]  # every rank sees every part, in rank order
-
-
-def test_batch_parts_combine_to_job_figures():
-    """5 instances dealt over 2 ranks: the job takes the slowest rank's wall
-    time, counts add, errors take the maximum, and the plain one-at-a-time
-    rate measured on rank 0 counts once per GPU."""
-    sys.path.insert(0, str(ROOT))
-    import bench
-    b = bench.combine_batch_parts([_part(0), _part(1)], 1000)
-    assert b["instances"] == 5 and b["ranks"] == 2 and b["cells"] == 5000
-    assert b["wall_s"] == 3.0 and b["solves_per_s"] == pytest.approx(5 / 3.0, abs=1e-3)
-    assert b["fp64_batch_solves_per_s"] == pytest.approx(1.0)
-    assert b["mcell_stage_per_s"] == pytest.approx(50_000 * 5 / 3.0 / 1e6, abs=0.1)
-    assert b["converged"] == 2 and b["nonphysical"] == 1 and b["mean_steps"] == pytest.approx(10.0)
-    assert b["cl_err_max"] == pytest.approx(2e-6) and b["cd_err_max"] == pytest.approx(2e-7)
-    assert b["within_1e-4"] == "4/5"
-    plain = b["plain_fp64_one_at_a_time"]
-    assert plain["solves_per_s_per_gpu"] == pytest.approx(0.5) and plain["solves_per_s_job"] == pytest.approx(1.0)
-    assert b["speedup_vs_plain"] == pytest.approx((5 / 3.0) / 1.0, abs=0.01)
-    assert b["p50_s"] == pytest.approx(2.0) and b["p99_s"] <= 3.0
+        assert parts == [{"rank": 0}, {"rank": 1}]  # every rank sees every part, in rank order
 
 
 def test_single_rank_needs_no_process_group():
@@ -92,18 +64,20 @@ def test_single_rank_needs_no_process_group():
     assert bench.replica_value(100, 2, 1.0, 1) == pytest.approx(100 * 5 * 2 / 1e-3 / 1e6)
 
 
-def test_serve_parts_combine_to_job_figures():
-    """Two ranks serving 3 + 2 requests: counts add, the slowest rank's wall
-    time is the job's, percentiles run over every request."""
+def test_stratified_sample_keeps_the_class_mix():
     sys.path.insert(0, str(ROOT))
     import bench
-    parts = [{"rate": 50.0, "requests": 3, "completed": 3, "converged": 1, "nonphysical": 0, "wall_s": 2.0,
-              "latencies": [0.1, 0.2, 0.3], "steps": [100, 200, 300]},
-             {"rate": 50.0, "requests": 2, "completed": 2, "converged": 2, "nonphysical": 1, "wall_s": 2.5,
-              "latencies": [0.4, 0.5], "steps": [400, 500]}]
-    j = bench.combine_serve_parts(parts)
-    assert j["ranks"] == 2 and j["requests"] == 5 and j["completed"] == 5
-    assert j["converged"] == 3 and j["nonphysical"] == 1
-    assert j["wall_s"] == 2.5 and j["solves_per_s"] == pytest.approx(2.0)
-    assert j["p50_s"] == pytest.approx(0.3) and 0.45 < j["p99_s"] <= 0.5
-    assert j["mean_steps"] == pytest.approx(300.0)
+    classes = ["a"] * 80 + ["b"] * 90 + ["c"] * 86
+    idx = bench.stratified_sample(classes, 24)
+    counts = {c: sum(1 for k in idx if classes[k] == c) for c in "abc"}
+    assert counts == {"a": 8, "b": 8, "c": 8}
+    assert idx == sorted(idx) and len(set(idx)) == len(idx)
+    assert bench.stratified_sample(["x"] * 3 + ["y"], 2) == [0, 1, 3]
+
+
+def test_thread_sweep_counts():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert bench.thread_counts(16) == [1, 2, 4, 8, 16]
+    assert bench.thread_counts(12) == [1, 2, 4, 8, 12]
+    assert bench.thread_counts(1) == [1]
