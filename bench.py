@@ -58,13 +58,20 @@ UNIT = "Mcell-stage/s"
 # Tile kernel: geometry = tau and n normals 32 B, V 8, 1/V 8, 1/d^2 8 = 56 B (FP64):
 #   split: stages 1-4: U 20 + U_n 40 + write 20 + geom 56 + ratio 4  = 140;  stage 5: 184;  average 148.8 B
 #   FP64:  stage 1: 144;  stages 2-4: 184;  stage 5: 192;  average 177.6 B
+# Paired-column marching kernel (split only, strips 56 wide): the same bytes,
+# except that the last stage takes V from the geometry record two rows back
+# instead of reading it again:
+#   split: 84, 104, 104, 104, last stage 172 - 4 = 168;  average 112.8 B
 BYTES_PER_STAGE = {("march", "split"): [84, 104, 104, 104, 172], ("march", "fp64"): [160, 200, 200, 200, 216],
+                   ("march2", "split"): [84, 104, 104, 104, 168],
                    ("tile", "split"): [140, 140, 140, 140, 184], ("tile", "fp64"): [144, 184, 184, 184, 192]}
+KERNEL_NAMES = {"march": "k_march", "march2": "k_march2", "tile": "k_stage"}
 
 
 def kernel_kind(kcfg) -> str:
-    """(tile_i, tile_j, threads) -> which stage kernel runs (strips are 26 wide)."""
-    return "march" if kcfg[1] == 26 else "tile"
+    """(tile_i, tile_j, threads) -> which stage kernel runs (strips are 26
+    wide, paired-column strips 56)."""
+    return {26: "march", 56: "march2"}.get(kcfg[1], "tile")
 
 
 def bytes_per_cell_stage(kind: str, prec: str) -> float:
@@ -306,7 +313,8 @@ def run_ours(args, world, rank, local):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if args.precision == "split" else "f64", "data": "synthetic",
             "config": {"workload": args.workload, "cells": cells, "precision": args.precision,
-                       "path": ("warp-marching strip" if kernel_kind(kcfg) == "march" else "tiled") +
+                       "path": {"march": "warp-marching strip", "march2": "paired-column warp-marching strip",
+                                "tile": "tiled"}[kernel_kind(kcfg)] +
                                " stage kernel, one launch per RK stage, CUDA graph per RK step",
                        "tile": "x".join(map(str, kcfg)) + (" (autotuned)" if not args.tile else ""),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -323,7 +331,7 @@ def run_ours(args, world, rank, local):
         line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                             "traffic": None if trafc is None else round(trafc * cells),
-                            "kernel": ("k_march" if kind == "march" else "k_stage") +
+                            "kernel": KERNEL_NAMES[kind] +
                                       " (5 launches per step; stage times " +
                                       ", ".join(f"{x:.3f}" for x in stage_ms) + " ms)",
                             "bytes_per_cell_stage": round(bps, 1)}

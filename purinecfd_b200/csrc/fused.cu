@@ -25,6 +25,7 @@
 #include "engine.h"
 #include "fused_kernels.cuh"
 #include "march_kernels.cuh"
+#include "march2_kernels.cuh"
 
 namespace jst {
 
@@ -148,8 +149,14 @@ void launch_wall_force(const Geom& g, const UnPtrs& up, const PhysConst& c, doub
 #define JST_FOR_TILES(X) X(4, 32, 256) X(8, 32, 256) X(16, 32, 256) X(4, 64, 256) X(8, 64, 256) X(8, 32, 192) X(8, 32, 128) X(16, 32, 384)
 // Marching-strip configurations: threads per block.  A strip is
 // fused::MARCH_W = 26 columns wide, so these are selected by tile_j == 26;
-// tile_i is the (maximum) strip height, a run-time choice.
+// tile_i is the (maximum) strip height, a run-time choice.  The paired-column
+// strips of the split precision (k_march2) are fused::MARCH2_W = 56 columns
+// wide: tile_j == 56.
 #define JST_FOR_MARCH(X) X(64) X(128) X(256)
+#define JST_FOR_MARCH2(X) X(64) X(128)
+
+// Strip width of a strip configuration (0 for a tile configuration).
+inline int strip_width(int tj) { return tj == fused::MARCH_W || tj == fused::MARCH2_W ? tj : 0; }
 
 template <class T> struct Kernels {
     void (*stage[3])(const TileRef*, int*, const Inst<T>*, int, double) = {nullptr, nullptr, nullptr};
@@ -187,6 +194,21 @@ template <class T, int NT> Kernels<T> march_kernels_for() {
     return k;
 }
 
+template <class T, int NT> Kernels<T> march2_kernels_for() {
+    Kernels<T> k;
+    if constexpr (std::is_same<T, float>::value) {
+        k.stage[0] = fused::k_march2<NT, true, false>;
+        k.stage[1] = fused::k_march2<NT, false, false>;
+        k.stage[2] = fused::k_march2<NT, false, true>;
+        k.dump = fused::k_march2<NT, true, false, true>;
+        k.step_dt = fused::k_step_dt<T, NT>;
+        k.smem = fused::march2_smem_bytes<NT>();
+        k.nt = NT;
+        k.march = true;
+    }
+    return k;
+}
+
 template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 256) {
 #define JST_PICK(a, b, n)                               \
     if (ti == a && tj == b && nt == n) {                \
@@ -202,12 +224,32 @@ template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 2
     }
     JST_FOR_MARCH(JST_PICK_MARCH)
 #undef JST_PICK_MARCH
+    if constexpr (std::is_same<T, float>::value) {
+#define JST_PICK_MARCH2(n)                                           \
+    if (ti >= 4 && ti <= 1024 && tj == fused::MARCH2_W && nt == n) { \
+        *out = march2_kernels_for<T, n>();                           \
+        return true;                                                 \
+    }
+        JST_FOR_MARCH2(JST_PICK_MARCH2)
+#undef JST_PICK_MARCH2
+    }
     return false;
 }
 
 template <class T> void build_march_geom(const Geom& g, int ni, int nj, T* rec, cudaStream_t st) {
     long n = (long)(ni + 1) * nj;
     JST_LAUNCH(fused::k_march_geom<T>, (unsigned)((n + 255) / 256), 256, 0, st, g.tnx, g.tny, g.nnx, g.nny, g.inv_vol,
+               g.inv_d2, g.vol, ni, nj, rec);
+}
+
+// Bytes of the paired-column geometry records (split precision only).
+template <class T> size_t march2_geom_bytes(int ni, int nj) {
+    return std::is_same<T, float>::value ? (size_t)(ni + 1) * fused::mg2_pairs(nj) * fused::M2_N * sizeof(float) : 0;
+}
+
+void build_march_geom2(const Geom& g, int ni, int nj, float* rec, cudaStream_t st) {
+    long n = (long)(ni + 1) * fused::mg2_pairs(nj);
+    JST_LAUNCH(fused::k_march_geom2, (unsigned)((n + 255) / 256), 256, 0, st, g.tnx, g.tny, g.nnx, g.nny, g.inv_vol,
                g.inv_d2, g.vol, ni, nj, rec);
 }
 
@@ -266,8 +308,8 @@ std::vector<TileRef> make_tiles(int inst, int ni, int nj, int ti, int tj) {
     t.reserve((size_t)a_n * b_n);
     for (int a = 0; a < a_n; ++a) {
         // marching strips: a_n bands of nearly equal height (at most ti rows)
-        int i0 = tj == fused::MARCH_W ? (int)((long)a * ni / a_n) : a * ti;
-        int i1 = tj == fused::MARCH_W ? (int)((long)(a + 1) * ni / a_n) : std::min(a * ti + ti, ni);
+        int i0 = strip_width(tj) ? (int)((long)a * ni / a_n) : a * ti;
+        int i1 = strip_width(tj) ? (int)((long)(a + 1) * ni / a_n) : std::min(a * ti + ti, ni);
         for (int b = 0; b < b_n; ++b) t.push_back(TileRef{inst, i0, b * tj, a * b_n + b, i1});
     }
     return t;
@@ -286,14 +328,15 @@ int tuned_tiles_bound(int ni, int nj) {
 // from a counter, so a launch lasts about ceil(strips / resident warps)
 // strip walks of (rows + 6) rows each.  Returns the height in [8, 128] that
 // minimises that over the given instances (nearly equal bands per instance).
-int march_height(const std::vector<std::pair<int, std::pair<int, int>>>& insts, long resident_warps) {
+int march_height(const std::vector<std::pair<int, std::pair<int, int>>>& insts, long resident_warps,
+                 int width = fused::MARCH_W) {
     int best_h = 32;
     double best = 1e300;
     for (int h = 8; h <= 128; ++h) {
         long strips = 0;
         double rows = 0.0;
         for (const auto& in : insts) {
-            long cols = (in.second.second + fused::MARCH_W - 1) / fused::MARCH_W;
+            long cols = (in.second.second + width - 1) / width;
             long bands = (in.second.first + h - 1) / h;
             strips += bands * cols;
             rows += (double)in.second.first * cols;
@@ -309,18 +352,20 @@ int march_height(const std::vector<std::pair<int, std::pair<int, int>>>& insts, 
     return best_h;
 }
 
-// The marching configuration the wave model picks for the given instances
-// (64 threads per block), without timing anything.
-template <class T> TuneResult model_choice(const std::vector<std::pair<int, std::pair<int, int>>>& insts) {
-    TuneResult r{32, fused::MARCH_W, 64, 0.f};
+// The marching configuration of strip width `width` (26: k_march, 56:
+// k_march2) the wave model picks for the given instances (64 threads per
+// block), without timing anything.
+template <class T>
+TuneResult model_choice(const std::vector<std::pair<int, std::pair<int, int>>>& insts, int width = fused::MARCH_W) {
+    TuneResult r{32, width, 64, 0.f};
     Kernels<T> K;
     int dev = 0, sms = 148, occ = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (pick_kernels<T>(32, fused::MARCH_W, &K, 64) &&
+    if (pick_kernels<T>(32, width, &K, 64) &&
         cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K.stage[1], K.nt, K.smem) == cudaSuccess)
-        r.ti = march_height(insts, (long)sms * std::max(1, occ) * (K.nt / 32));
+        r.ti = march_height(insts, (long)sms * std::max(1, occ) * (K.nt / 32), width);
     cudaGetLastError();
     return r;
 }
@@ -355,6 +400,11 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
         for (const auto& cd : kTileCands) cands.push_back({cd[0], cd[1], cd[2]});
         cands.push_back({m.ti, m.tj, 64});
         cands.push_back({m.ti, m.tj, 128});
+    }
+    if (std::is_same<T, float>::value) {  // paired-column strips
+        const TuneResult m2 = model_choice<T>(insts, fused::MARCH2_W);
+        cands.push_back({m2.ti, m2.tj, 64});
+        if (total_cells(insts) >= kTuneMinCells) cands.push_back({m2.ti, m2.tj, 128});
     }
     for (const auto& cand : cands) {
         Kernels<T> K;
@@ -509,6 +559,7 @@ template <class T> class FusedEngine : public Engine {
         size_t o_hist = add(hist_cap_ * sizeof(double));
         size_t o_field = add(n * sizeof(double));
         size_t o_mg = add((size_t)(ni + 1) * nj * fused::MG_N * sizeof(T));
+        size_t o_mg2 = add(march2_geom_bytes<T>(ni, nj));
         if (cudaMalloc(&arena_, bytes) != cudaSuccess) {
             err = "cudaMalloc failed for the fused-path state (" + std::to_string(bytes >> 20) + " MiB)";
             return false;
@@ -541,6 +592,7 @@ template <class T> class FusedEngine : public Engine {
         I.res_hist = reinterpret_cast<double*>(base + o_hist);
         I.st = reinterpret_cast<InstState*>(base + o_st);
         I.c = C.c;
+        I.cp = fused::make_constp(C.c);
         inst_ = I;
         d_inst_ = reinterpret_cast<Inst<T>*>(base + o_inst);
         d_tiles_ = reinterpret_cast<TileRef*>(base + o_tiles);
@@ -549,6 +601,7 @@ template <class T> class FusedEngine : public Engine {
         d_unptr_ = reinterpret_cast<double**>(base + o_unptr);
         d_field_ = reinterpret_cast<double*>(base + o_field);
         inst_.mg = reinterpret_cast<T*>(base + o_mg);
+        inst_.mg2 = march2_geom_bytes<T>(ni, nj) ? reinterpret_cast<float*>(base + o_mg2) : nullptr;
         cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_ntiles_, &ntiles_, sizeof(int), cudaMemcpyHostToDevice, C.st);
@@ -559,6 +612,7 @@ template <class T> class FusedEngine : public Engine {
         }
         JST_LAUNCH(k_far_geom, (nj + 255) / 256, 256, 0, C.st, C.g, const_cast<double*>(inst_.far));
         build_march_geom(C.g, ni, nj, const_cast<T*>(inst_.mg), C.st);
+        if (inst_.mg2) build_march_geom2(C.g, ni, nj, const_cast<float*>(inst_.mg2), C.st);
         return cudaGetLastError() == cudaSuccess;
     }
 
@@ -1264,6 +1318,7 @@ template <class T> class Batch : public BatchBase {
         add(2 * (size_t)ntiles * sizeof(double));    // partials
         add(5 * (size_t)nt * sizeof(double));        // far
         add(ntau * fused::MG_N * sizeof(T));         // marching geometry records
+        add(march2_geom_bytes<T>(nr - 1, nt));       // paired-column records (split)
         return b;
     }
 
@@ -1363,13 +1418,17 @@ template <class T> class Batch : public BatchBase {
             double* far = reinterpret_cast<double*>(take(5 * (size_t)nj * sizeof(double)));
             I.far = far;
             I.mg = reinterpret_cast<T*>(take((size_t)(ni + 1) * nj * fused::MG_N * sizeof(T)));
+            I.mg2 = march2_geom_bytes<T>(ni, nj) ? reinterpret_cast<float*>(take(march2_geom_bytes<T>(ni, nj)))
+                                                 : nullptr;
             I.res_hist = nullptr;
             I.st = d_states_ + slot;
             I.c = c;
+            I.cp = fused::make_constp(c);
             cudaMemcpyAsync(d_xy, p.xy.data(), p.xy.size() * sizeof(double), cudaMemcpyHostToDevice, st_);
             geometry_build(d_xy, p.n_rings, nj, g, st_);
             JST_LAUNCH(k_far_geom, (nj + 255) / 256, 256, 0, st_, g, far);
             build_march_geom(g, ni, nj, const_cast<T*>(I.mg), st_);
+            if (I.mg2) build_march_geom2(g, ni, nj, const_cast<float*>(I.mg2), st_);
             JST_LAUNCH(k_fill_freestream, (unsigned)((n + 255) / 256), 256, 0, st_, I.un[0], I.un[1], I.un[2],
                        I.un[3], I.un[4], (long)n, c);
             InstState s0{};

@@ -62,6 +62,64 @@ struct InstState {
     int pad;
 };
 
+// The per-instance constants of the split precision's paired-column kernel,
+// rounded once to FP32 and stored as pairs (both halves equal), so that a
+// use is one 64-bit load: the kernel copies them to shared memory per strip.
+// The f_w constants stay FP64 (fw_of_f32 forms g in FP64).
+struct ConstP {
+    float2 inv_t_ref, suth_num, t_suth, cv1_cubed, inv_pr, inv_prt, cp, sigma;
+    float2 inv_kappa2, m_ct4, ct3, fv3, cb1, rmax, cw1, m_cb1_k2, cb2_sigma, rg, cfl;
+    float2 gm1, r_gas, half_cfl, k2, k4, p_ref2;
+    float2 f_rho, f_p, f_t, f_vx, f_vy, f_e, f_nut, pad;
+    double cw2, cw3_6, one_plus_cw3_6, fw_lim;
+};
+
+JST_HD ConstP make_constp(const PhysConst& c) {
+    auto s = [](double x) {
+        float f = (float)x;
+        return float2{f, f};
+    };
+    ConstP k;
+    k.inv_t_ref = s(c.inv_t_ref);
+    k.suth_num = s(c.suth_num);
+    k.t_suth = s(c.t_suth);
+    k.cv1_cubed = s(c.cv1_cubed);
+    k.inv_pr = s(c.inv_pr);
+    k.inv_prt = s(c.inv_prt);
+    k.cp = s(c.cp);
+    k.sigma = s(c.sigma);
+    k.inv_kappa2 = s(c.inv_kappa2);
+    k.m_ct4 = s(-c.Ct4);
+    k.ct3 = s(c.Ct3);
+    k.fv3 = s(c.fv3);
+    k.cb1 = s(c.Cb1);
+    k.rmax = s(c.rmax);
+    k.cw1 = s(c.cw1);
+    k.m_cb1_k2 = s(-c.cb1_k2);
+    k.cb2_sigma = s(c.cb2_sigma);
+    k.rg = s(c.rg);
+    k.cfl = s(c.cfl);
+    k.gm1 = s(c.gm1);
+    k.r_gas = s(c.r_gas);
+    k.half_cfl = s(c.half_cfl);
+    k.k2 = s(c.k2);
+    k.k4 = s(c.k4);
+    k.p_ref2 = s(2.0 * c.p_inf);
+    k.f_rho = s(c.f_rho);
+    k.f_p = s(c.f_p);
+    k.f_t = s(c.f_t);
+    k.f_vx = s(c.f_vx);
+    k.f_vy = s(c.f_vy);
+    k.f_e = s(c.f_e);
+    k.f_nut = s(c.f_nut);
+    k.pad = s(0.0);
+    k.cw2 = c.Cw2;
+    k.cw3_6 = c.cw3_6;
+    k.one_plus_cw3_6 = c.one_plus_cw3_6;
+    k.fw_lim = c.fw_lim;
+    return k;
+}
+
 // Per-instance descriptor (read-only during a launch except through `st`).
 template <class T> struct Inst {
     int ni, nj;
@@ -86,6 +144,10 @@ template <class T> struct Inst {
     // {tau nx, ny of face row k; n nx, ny, 1/V, 1/d^2, V of cell row k-1; 0}
     // in the stage type (zeros for cell row -1), see k_march_geom
     const T* mg;
+    // paired-column marching kernel (split precision): the same records with
+    // the two columns of each pair interleaved, see k_march_geom2
+    const float* mg2;
+    ConstP cp;  // make_constp(c)
     // residual dump (jst_stage_residual): 5 planes of NI*NJ doubles that the
     // DUMP instantiation of stage 0 writes R = Fc - Fv - Fd - S into
     double* rdump;

@@ -211,8 +211,27 @@ template <class T> struct MarchURing {
     T u[5][5][32];  // [row slot][variable][lane]
 };
 
-template <class T, int NT, bool PIPE> constexpr size_t march_smem_bytes() {
+// Per warp: the row buffers, the U ring (FP64) and a copy of the strip's
+// instance constants (PhysConst), read by every row of the walk; in shared
+// memory a constant costs a short-latency load instead of a global one.
+JST_HD constexpr size_t march_const_bytes() { return (sizeof(PhysConst) + 15) / 16 * 16; }
+template <class T, int NT, bool PIPE> JST_HD constexpr size_t march_buf_bytes() {
     return (size_t)(NT / 32) * ((PIPE ? 2 * sizeof(MarchRow<T>) : 0) + (march_u_ring<T>() ? sizeof(MarchURing<T>) : 0));
+}
+template <class T, int NT, bool PIPE> JST_HD constexpr size_t march_smem_bytes() {
+    return march_buf_bytes<T, NT, PIPE>() + (size_t)(NT / 32) * march_const_bytes();
+}
+
+// Copies the instance constants into this warp's slot (8-byte words, one per
+// lane), between warp barriers so that the previous strip's reads are done.
+JST_D void warp_copy_const(PhysConst* dst, const PhysConst* src) {
+#ifdef __CUDA_ARCH__
+    __syncwarp();
+    const unsigned long long* s8 = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* d8 = reinterpret_cast<unsigned long long*>(dst);
+    for (int w = JST_LANE(); w < (int)(sizeof(PhysConst) / 8); w += 32) d8[w] = s8[w];
+    __syncwarp();
+#endif
 }
 
 // Minimum resident blocks per SM asked of the register allocator: 12 warps
@@ -245,13 +264,13 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
     constexpr bool ACC32 = sizeof(T) == sizeof(float) && !LAST;
     MarchRow<T>* rowbuf = nullptr;
     MarchURing<T>* uring = nullptr;
-    if constexpr (PIPE || UR) {
-        JST_DYN_SMEM(smem_raw);
-        const int w = JST_WARP_IN_BLOCK();
-        if constexpr (PIPE) rowbuf = reinterpret_cast<MarchRow<T>*>(smem_raw) + 2 * w;
-        if constexpr (UR)
-            uring = reinterpret_cast<MarchURing<T>*>(smem_raw + (PIPE ? (size_t)(NT / 32) * 2 * sizeof(MarchRow<T>) : 0)) + w;
-    }
+    JST_DYN_SMEM(smem_raw);
+    const int wib = JST_WARP_IN_BLOCK();
+    if constexpr (PIPE) rowbuf = reinterpret_cast<MarchRow<T>*>(smem_raw) + 2 * wib;
+    if constexpr (UR)
+        uring = reinterpret_cast<MarchURing<T>*>(smem_raw + (PIPE ? (size_t)(NT / 32) * 2 * sizeof(MarchRow<T>) : 0)) + wib;
+    PhysConst* cwarp =
+        reinterpret_cast<PhysConst*>(smem_raw + march_buf_bytes<T, NT, PIPE>() + (size_t)wib * march_const_bytes());
     const int nt_all = sched[0];
     unsigned* work = reinterpret_cast<unsigned*>(sched + 1);
     unsigned* exitc = reinterpret_cast<unsigned*>(sched + 2);
@@ -270,7 +289,8 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         const TileRef tr = tiles[ticket];
         const Inst<T>& I = insts[tr.inst];
         const int ni = I.ni, nj = I.nj, i0 = tr.i0, j0 = tr.j0;
-        const PhysConst& c = I.c;
+        warp_copy_const(cwarp, &I.c);
+        const PhysConst& c = *cwarp;
 
         int hdr[3] = {0, 0, 0};  // skip, fresh, step
         if (lane == 0) {
