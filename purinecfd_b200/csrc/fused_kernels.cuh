@@ -62,16 +62,16 @@ struct InstState {
     int pad;
 };
 
-// The per-instance constants of the split precision's paired-column kernel,
-// rounded once to FP32 and stored as pairs (both halves equal), so that a
-// use is one 64-bit load: the kernel copies them to shared memory per strip.
-// The f_w constants stay FP64 (fw_of_f32 forms g in FP64).
+// The per-instance constants of the split precision's marching kernels,
+// rounded once to FP32 and stored as pairs (both halves equal): the
+// paired-column kernel reads a pair with one 64-bit load, the one-column
+// kernel the first half; both copy them to shared memory per strip.
 struct ConstP {
     float2 inv_t_ref, suth_num, t_suth, cv1_cubed, inv_pr, inv_prt, cp, sigma;
     float2 inv_kappa2, m_ct4, ct3, fv3, cb1, rmax, cw1, m_cb1_k2, cb2_sigma, rg, cfl;
     float2 gm1, r_gas, half_cfl, k2, k4, p_ref2;
-    float2 f_rho, f_p, f_t, f_vx, f_vy, f_e, f_nut, pad;
-    double cw2, cw3_6, one_plus_cw3_6, fw_lim;
+    float2 f_rho, f_p, f_t, f_vx, f_vy, f_e, f_nut;
+    float2 cw2, cw3_6, one_plus_cw3_6, fw_lim;
 };
 
 JST_HD ConstP make_constp(const PhysConst& c) {
@@ -112,11 +112,10 @@ JST_HD ConstP make_constp(const PhysConst& c) {
     k.f_vy = s(c.f_vy);
     k.f_e = s(c.f_e);
     k.f_nut = s(c.f_nut);
-    k.pad = s(0.0);
-    k.cw2 = c.Cw2;
-    k.cw3_6 = c.cw3_6;
-    k.one_plus_cw3_6 = c.one_plus_cw3_6;
-    k.fw_lim = c.fw_lim;
+    k.cw2 = s(c.Cw2);
+    k.cw3_6 = s(c.cw3_6);
+    k.one_plus_cw3_6 = s(c.one_plus_cw3_6);
+    k.fw_lim = s(c.fw_lim);
     return k;
 }
 

@@ -339,6 +339,18 @@ JST_HD float fw_of_f32(float r, double cw2, double cw3_6, double one_plus_cw3_6,
     return g > 1e5 ? (float)fw_lim : v;
 }
 
+// fw for the FP32 path without FP64: r is clamped at -1e4 before r^6 is
+// formed (r^6 <= 1e24 fits FP32); below the clamp g = r + Cw2 (r^6 - r) is
+// beyond 1e5 either way, where fw takes its limit, so the clamp changes no
+// result.  Otherwise as fw_of_f32.
+JST_HD float fw_f32(float r, float cw2, float cw3_6, float one_plus_cw3_6, float fw_lim) {
+    const float rc = fmaxf(r, -1e4f);
+    const float g = rc + cw2 * (powi6<float>(rc) - rc);
+    const float gf = fminf(g, 1e5f);  // NaN passes through
+    const float v = gf * root6_f32(one_plus_cw3_6 / (powi6<float>(gf) + cw3_6));
+    return g > 1e5f ? fw_lim : v;
+}
+
 // source::compute for one cell (source.rs:55-85), before the factor V.
 template <class T, bool Q = false>
 JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny, const PhysConst& c) {
@@ -353,7 +365,8 @@ JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T 
     T prod = T(c.Cb1) * (T(1) - ft2) * s_tilde * rho_nu;
     T r = tmin<T>(dv<T, Q>(nu_tilde, s_tilde) * inv_kd2, T(c.rmax));
     T fw;
-    if constexpr (sizeof(T) == sizeof(float)) fw = fw_of_f32(r, c.Cw2, c.cw3_6, c.one_plus_cw3_6, c.fw_lim);
+    if constexpr (sizeof(T) == sizeof(float))
+        fw = fw_f32(r, (float)c.Cw2, (float)c.cw3_6, (float)c.one_plus_cw3_6, (float)c.fw_lim);
     else fw = fw_of<T, Q>(r, T(c.Cw2), T(c.cw3_6), T(c.one_plus_cw3_6), T(c.fw_lim));
     T destr = (T(c.cw1) * fw - T(c.cb1_k2) * ft2) * rho * (nu_tilde * nu_tilde * inv_dist2);
     T diff = T(c.cb2_sigma) * rho * (dnx * dnx + dny * dny);

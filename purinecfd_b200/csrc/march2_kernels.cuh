@@ -233,8 +233,7 @@ JST_D Diff2 diffusion2(P2 t, P2 rho_nu, P2 vx, P2 vy, const P2* g, const ConstP&
     o.d[7] = nu_diff * g[7];
     return o;
 }
-// source::compute for both cells (source.rs:55-85), before the factor V;
-// f_w per element from an FP64 g (fw_of_f32)
+// source::compute for both cells (source.rs:55-85), before the factor V
 JST_D P2 sa_source2(P2 rho, P2 rho_nu, P2 inv_d2, P2 chi, P2 f1, P2 dvdx, P2 dudy, P2 dnx, P2 dny,
                     const ConstP& K) {
     const P2 nu_t = pdiv(rho_nu, rho);
@@ -246,8 +245,15 @@ JST_D P2 sa_source2(P2 rho, P2 rho_nu, P2 inv_d2, P2 chi, P2 f1, P2 dvdx, P2 dud
     const P2 s_t = pmax(pfma(nu_t * inv_kd2, fv2, sv), sp(1e-10f));
     const P2 prod = P2{K.cb1} * (sp(1.0f) - ft2) * s_t * rho_nu;
     const P2 r = pmin(pdiv(nu_t, s_t) * inv_kd2, P2{K.rmax});
-    const P2 fw = p2(fw_of_f32(r.v.x, K.cw2, K.cw3_6, K.one_plus_cw3_6, K.fw_lim),
-                     fw_of_f32(r.v.y, K.cw2, K.cw3_6, K.one_plus_cw3_6, K.fw_lim));
+    // fw as fw_f32 (jst_common.cuh), paired
+    const P2 rc = pmax(r, sp(-1e4f));
+    const P2 r2 = rc * rc;
+    const P2 g = pfma(P2{K.cw2}, r2 * r2 * r2 - rc, rc);
+    const P2 gf = pmin(g, sp(1e5f));
+    const P2 g2 = gf * gf;
+    const P2 q = pdiv(P2{K.one_plus_cw3_6}, pfma(g2 * g2, g2, P2{K.cw3_6}));
+    const P2 v = gf * p2(root6_f32(q.v.x), root6_f32(q.v.y));
+    const P2 fw = psel(g.v.x > 1e5f, g.v.y > 1e5f, P2{K.fw_lim}, v);
     const P2 destr = pfma(P2{K.cw1}, fw, P2{K.m_cb1_k2} * ft2) * rho * (nu_t * nu_t * inv_d2);
     const P2 diff = P2{K.cb2_sigma} * rho * pfma(dnx, dnx, dny * dny);
     return prod - destr + diff;

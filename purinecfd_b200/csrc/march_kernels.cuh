@@ -212,9 +212,11 @@ template <class T> struct MarchURing {
 };
 
 // Per warp: the row buffers, the U ring (FP64) and a copy of the strip's
-// instance constants (PhysConst), read by every row of the walk; in shared
-// memory a constant costs a short-latency load instead of a global one.
-JST_HD constexpr size_t march_const_bytes() { return (sizeof(PhysConst) + 15) / 16 * 16; }
+// instance constants (PhysConst, and for the FP32 arithmetic ConstP), read
+// by every row of the walk; in shared memory a constant costs a
+// short-latency load instead of a global one (and in FP32 no conversion).
+JST_HD constexpr size_t march_phys_bytes() { return (sizeof(PhysConst) + 15) / 16 * 16; }
+JST_HD constexpr size_t march_const_bytes() { return march_phys_bytes() + (sizeof(ConstP) + 15) / 16 * 16; }
 template <class T, int NT, bool PIPE> JST_HD constexpr size_t march_buf_bytes() {
     return (size_t)(NT / 32) * ((PIPE ? 2 * sizeof(MarchRow<T>) : 0) + (march_u_ring<T>() ? sizeof(MarchURing<T>) : 0));
 }
@@ -222,16 +224,41 @@ template <class T, int NT, bool PIPE> JST_HD constexpr size_t march_smem_bytes()
     return march_buf_bytes<T, NT, PIPE>() + (size_t)(NT / 32) * march_const_bytes();
 }
 
-// Copies the instance constants into this warp's slot (8-byte words, one per
-// lane), between warp barriers so that the previous strip's reads are done.
-JST_D void warp_copy_const(PhysConst* dst, const PhysConst* src) {
+// Copies an instance's constants into this warp's slot (8-byte words, one
+// per lane), between warp barriers so that the previous strip's reads are
+// done.
+template <class C> JST_D void warp_copy_const(C* dst, const C* src) {
 #ifdef __CUDA_ARCH__
     __syncwarp();
     const unsigned long long* s8 = reinterpret_cast<const unsigned long long*>(src);
     unsigned long long* d8 = reinterpret_cast<unsigned long long*>(dst);
-    for (int w = JST_LANE(); w < (int)(sizeof(PhysConst) / 8); w += 32) d8[w] = s8[w];
+    for (int w = JST_LANE(); w < (int)(sizeof(C) / 8); w += 32) d8[w] = s8[w];
     __syncwarp();
 #endif
+}
+
+// A constant in the stage arithmetic: the FP32 copy for T = float, the FP64
+// value otherwise.
+template <class T> JST_D T kc(double d, float2 f) {
+    if constexpr (sizeof(T) == sizeof(float)) return f.x;
+    else return d;
+}
+
+// source::compute for one cell in FP32 (sa_source) from the FP32 constants.
+JST_D float sa_source_f32(float rho, float rho_nu, float inv_dist2, float chi, float f1, float dvdx, float dudy,
+                          float dnx, float dny, const ConstP& K) {
+    const float nu_tilde = rho_nu / rho;
+    const float inv_kd2 = inv_dist2 * K.inv_kappa2.x;
+    const float ft2 = K.ct3.x * exp_f32(K.m_ct4.x * chi * chi);
+    const float fv2 = 1.0f - chi / (1.0f + chi * f1);
+    const float sv = K.fv3.x * fabsf(dvdx - dudy);
+    const float s_tilde = fmaxf(sv + nu_tilde * inv_kd2 * fv2, 1e-10f);
+    const float prod = K.cb1.x * (1.0f - ft2) * s_tilde * rho_nu;
+    const float r = fminf(nu_tilde / s_tilde * inv_kd2, K.rmax.x);
+    const float fw = fw_f32(r, K.cw2.x, K.cw3_6.x, K.one_plus_cw3_6.x, K.fw_lim.x);
+    const float destr = (K.cw1.x * fw + K.m_cb1_k2.x * ft2) * rho * (nu_tilde * nu_tilde * inv_dist2);
+    const float diff = K.cb2_sigma.x * rho * (dnx * dnx + dny * dny);
+    return prod - destr + diff;
 }
 
 // Minimum resident blocks per SM asked of the register allocator: 12 warps
@@ -271,6 +298,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         uring = reinterpret_cast<MarchURing<T>*>(smem_raw + (PIPE ? (size_t)(NT / 32) * 2 * sizeof(MarchRow<T>) : 0)) + wib;
     PhysConst* cwarp =
         reinterpret_cast<PhysConst*>(smem_raw + march_buf_bytes<T, NT, PIPE>() + (size_t)wib * march_const_bytes());
+    ConstP* kwarp = reinterpret_cast<ConstP*>(reinterpret_cast<unsigned char*>(cwarp) + march_phys_bytes());
     const int nt_all = sched[0];
     unsigned* work = reinterpret_cast<unsigned*>(sched + 1);
     unsigned* exitc = reinterpret_cast<unsigned*>(sched + 2);
@@ -290,7 +318,9 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         const Inst<T>& I = insts[tr.inst];
         const int ni = I.ni, nj = I.nj, i0 = tr.i0, j0 = tr.j0;
         warp_copy_const(cwarp, &I.c);
+        if constexpr (sizeof(T) == sizeof(float)) warp_copy_const(kwarp, &I.cp);
         const PhysConst& c = *cwarp;
+        const ConstP& K = *kwarp;
 
         int hdr[3] = {0, 0, 0};  // skip, fresh, step
         if (lane == 0) {
@@ -329,11 +359,11 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         const int gj = wrapj(cu, nj);
         const bool seam = cu < 0 || cu >= nj;
         const bool out_lane = lane >= 3 && lane < 3 + MARCH_W && cu < nj;
-        const T gm1 = (T)c.gm1, rgas = (T)c.r_gas;
-        const T half_cfl = (T)c.half_cfl, k2 = (T)c.k2, k4 = (T)c.k4;
+        const T gm1 = kc<T>(c.gm1, K.gm1), rgas = kc<T>(c.r_gas, K.r_gas);
+        const T half_cfl = kc<T>(c.half_cfl, K.half_cfl), k2 = kc<T>(c.k2, K.k2), k4 = kc<T>(c.k4, K.k4);
         // face fluxes are formed from twice the face state (see face_combine),
         // so the pressure reference of euler_flux is doubled as well
-        const T p_ref2 = sizeof(T) == sizeof(double) ? T(0) : (T)(2.0 * c.p_inf);
+        const T p_ref2 = sizeof(T) == sizeof(double) ? T(0) : kc<T>(0.0, K.p_ref2);
 
         // PIPE: stage the global inputs that row kk of the walk reads.  The
         // conditions are the ones under which the walk reads them.
@@ -435,13 +465,13 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 for (int v = 0; v < 5; ++v) uk[v] = PIPE ? B->u[v][lane] : ld(src + v * np + id);
                 Prim<T> p;
                 if (fresh) {
-                    p.rho = (T)c.f_rho;
-                    p.p = (T)c.f_p;
-                    p.t = (T)c.f_t;
-                    p.vx = (T)c.f_vx;
-                    p.vy = (T)c.f_vy;
-                    p.e = (T)c.f_e;
-                    p.nut = (T)c.f_nut;
+                    p.rho = kc<T>(c.f_rho, K.f_rho);
+                    p.p = kc<T>(c.f_p, K.f_p);
+                    p.t = kc<T>(c.f_t, K.f_t);
+                    p.vx = kc<T>(c.f_vx, K.f_vx);
+                    p.vy = kc<T>(c.f_vy, K.f_vy);
+                    p.e = kc<T>(c.f_e, K.f_e);
+                    p.nut = kc<T>(c.f_nut, K.f_nut);
                 } else {
                     p = unpack_cell<T, true>(uk[0], uk[1], uk[2], uk[3], uk[4], gm1, rgas);
                 }
@@ -454,7 +484,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     q.vx = -p.vx;
                     q.vy = -p.vy;
                     q.nut = -p.nut;
-                    q.e = fresh ? (T)c.f_e : uk[3] * dv<T, true>(T(1), q.rho);
+                    q.e = fresh ? kc<T>(c.f_e, K.f_e) : uk[3] * dv<T, true>(T(1), q.rho);
                     pack_cell<T>(q, uk);
                     p = q;
                 }
@@ -532,9 +562,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                                                  rty, iv, &g[2 * q], &g[2 * q + 1]);
                     }
                     Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], g[0], g[1], g[2],
-                                                          g[3], g[4], g[5], g[6], g[7], (T)c.inv_t_ref,
-                                                          (T)c.suth_num, (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr,
-                                                          (T)c.inv_prt, (T)c.cp, (T)c.sigma);
+                                                          g[3], g[4], g[5], g[6], g[7], kc<T>(c.inv_t_ref, K.inv_t_ref), kc<T>(c.suth_num, K.suth_num), kc<T>(c.t_suth, K.t_suth), kc<T>(c.cv1_cubed, K.cv1_cubed), kc<T>(c.inv_pr, K.inv_pr), kc<T>(c.inv_prt, K.inv_prt), kc<T>(c.cp, K.cp), kc<T>(c.sigma, K.sigma));
                     dn[0] = d.dx1;
                     dn[1] = d.dx2;
                     dn[2] = d.dx3;
@@ -544,17 +572,19 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     dn[6] = d.dy3;
                     dn[7] = d.dy4;
                     if (S || (r >= i0 && r < i1)) {
-                        T s5 = sa_source<T, true>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6],
-                                                  g[7], c);
+                        T s5;
+                        if constexpr (sizeof(T) == sizeof(float))
+                            s5 = sa_source_f32(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], K);
+                        else
+                            s5 = sa_source<T, true>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7],
+                                                    c);
                         snew = s5 * gk[MG_VOL];
                     }
                     if (!S && r == 0) {
                         // the wall ghost ring (row -1, one row up in the window) takes cell
                         // 0's gradient with grad T = 0 (gradient.rs:93-95)
                         Diff<T> w = diffusion_tensor<T, true>(qw[0][2], UA(2, 4), qw[0][0], qw[0][1], g[0], g[1],
-                                                              g[2], g[3], T(0), T(0), g[6], g[7], (T)c.inv_t_ref,
-                                                              (T)c.suth_num, (T)c.t_suth, (T)c.cv1_cubed,
-                                                              (T)c.inv_pr, (T)c.inv_prt, (T)c.cp, (T)c.sigma);
+                                                              g[2], g[3], T(0), T(0), g[6], g[7], kc<T>(c.inv_t_ref, K.inv_t_ref), kc<T>(c.suth_num, K.suth_num), kc<T>(c.t_suth, K.t_suth), kc<T>(c.cv1_cubed, K.cv1_cubed), kc<T>(c.inv_pr, K.inv_pr), kc<T>(c.inv_prt, K.inv_prt), kc<T>(c.cp, K.cp), kc<T>(c.sigma, K.sigma));
                         dw[1][0] = w.dx1;
                         dw[1][1] = w.dx2;
                         dw[1][2] = w.dx3;
@@ -566,9 +596,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     }
                 } else if (r >= ni) {  // far ghost ring: zero gradient (gradient.rs:96)
                     Diff<T> d = diffusion_tensor<T, true>(qw[1][2], UA(3, 4), qw[1][0], qw[1][1], T(0), T(0), T(0),
-                                                          T(0), T(0), T(0), T(0), T(0), (T)c.inv_t_ref,
-                                                          (T)c.suth_num, (T)c.t_suth, (T)c.cv1_cubed, (T)c.inv_pr,
-                                                          (T)c.inv_prt, (T)c.cp, (T)c.sigma);
+                                                          T(0), T(0), T(0), T(0), T(0), kc<T>(c.inv_t_ref, K.inv_t_ref), kc<T>(c.suth_num, K.suth_num), kc<T>(c.t_suth, K.t_suth), kc<T>(c.cv1_cubed, K.cv1_cubed), kc<T>(c.inv_pr, K.inv_pr), kc<T>(c.inv_prt, K.inv_prt), kc<T>(c.cp, K.cp), kc<T>(c.sigma, K.sigma));
                     dn[0] = d.dx1;
                     dn[1] = d.dx2;
                     dn[2] = d.dx3;
@@ -711,7 +739,8 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                         T dd = T(0.5) * (ny2[0] + nyr3);
                         T vol = PIPE ? B->volm[lane] : ld(I.mg + MG_N * (id + nj) + MG_VOL);
                         T qvx = (T)q.vx, qvy = (T)q.vy, qt = (T)q.t;
-                        T dl = local_dt<T, true>(qvx, qvy, sq<T, true>((T)c.rg * qt), aa, bb, cc, dd, (T)c.cfl * vol);
+                        T dl = local_dt<T, true>(qvx, qvy, sq<T, true>(kc<T>(c.rg, K.rg) * qt), aa, bb, cc, dd,
+                                                 kc<T>(c.cfl, K.cfl) * vol);
                         if (ok) {
                             ratio_next[id] = dv<T, true>(vol, dl);
                             if (dt_local) I.ldt[id] = (double)dl;
