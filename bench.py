@@ -294,9 +294,10 @@ def run_ours(args, world, rank, local):
         tile = {"tile_i": parts[0], "tile_j": parts[1]}
         if len(parts) > 2:
             tile["block_threads"] = parts[2]
-    s = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=local, **tile)
+    s = Solver(cfg, xy, nr, nt, precision=prec, kernel_path=PATH_FUSED, device=local, staging=args.staging, **tile)
     cells = s.n_cells
     kcfg = s.kernel_config()
+    kstg = s.kernel_staging()
     s.time_steps(args.warmup)
     barrier(world)
     with ClockSampler(local) as clk:
@@ -317,6 +318,7 @@ def run_ours(args, world, rank, local):
                                 "tile": "tiled"}[kernel_kind(kcfg)] +
                                " stage kernel, one launch per RK stage, CUDA graph per RK step",
                        "tile": "x".join(map(str, kcfg)) + (" (autotuned)" if not args.tile else ""),
+                       "staging": {0: None, 1: "per-lane cp.async", 2: "bulk cp.async.bulk (TMA)"}[kstg],
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (state + geometry ~0.7 GB)"},
             "gpu_launches": 5 * args.steps, "residual_after": residual}
@@ -553,6 +555,7 @@ def main():
     ap.add_argument("--workload", default="naca0012_4097x1025")
     ap.add_argument("--precision", choices=["split", "fp64"], default="split")
     ap.add_argument("--tile", default="", help="fused tile TIxTJ (default: the library's choice)")
+    ap.add_argument("--staging", type=int, default=0, help="marching-strip row staging: 0 auto, 1 per-lane, 2 bulk")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain-path line")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")

@@ -57,6 +57,16 @@ typedef enum {
     JST_DT_LOCAL = 1   /* each cell advances with its own CFL step (steady-state acceleration) */
 } jst_dt_mode;
 
+/* How the marching-strip stage kernels stage each row's inputs in shared
+ * memory (no counterpart in the reference).  Both give the same results. */
+typedef enum {
+    JST_STAGING_AUTO = 0,     /* the autotuner's choice (per-lane copies when the tile is given) */
+    JST_STAGING_PER_LANE = 1, /* one cp.async per lane and field */
+    JST_STAGING_BULK = 2      /* one cp.async.bulk (TMA) copy per field's row segment, completed on an
+                                 mbarrier with a bounded wait (rings whose width is not a multiple of
+                                 16 bytes, or under 36 columns, fall back to per-lane copies) */
+} jst_staging;
+
 /* Which kernels run a stage. */
 typedef enum {
     JST_PATH_FUSED = 0, /* one stage kernel per RK stage (production): warp-marching
@@ -74,6 +84,7 @@ typedef struct {
     int use_graph;   /* capture each RK step as a CUDA graph (fused path) */
     double nut_inf_ratio; /* free-stream nu-tilde / nu; <= 0 uses the config value or 0.1 */
     int block_threads;    /* fused path threads per block (0 = default for the tile) */
+    int staging;          /* jst_staging of the marching strips */
 } jst_opts;
 
 /* Fills opts with the defaults: FP64, global dt, fused path, device 0,
@@ -238,6 +249,7 @@ typedef struct {
     double hbm_budget_gb; /* device memory the batch may hold for instances */
     int keep_fields;      /* copy U of retired instances to host memory */
     int block_threads;    /* threads per block (0 = default for the tile) */
+    int staging;          /* jst_staging of the marching strips */
 } jst_batch_opts;
 
 void jst_batch_default_opts(jst_batch_opts* o);
@@ -262,6 +274,11 @@ jst_status jst_batch_step(jst_batch* b, int nsteps);
  * the options or, when those are 0, by the autotuner at the first
  * jst_batch_step (tile_j == 26: marching strips of at most tile_i rows). */
 jst_status jst_batch_kernel_config(const jst_batch* b, int* tile_i, int* tile_j, int* block_threads);
+
+/* jst_staging the batch's stage kernel runs with (0 when it is not a
+ * marching strip).  A bounded row-copy wait that runs out makes
+ * jst_batch_step fail with JST_ERR_TIMEOUT. */
+jst_status jst_batch_kernel_staging(const jst_batch* b, int* staging);
 
 /* Counts of active and queued instances and device bytes in use. */
 jst_status jst_batch_stats(jst_batch* b, int* active, int* queued, double* bytes_in_use);
@@ -307,6 +324,11 @@ jst_status jst_residual_noalloc(const double* rho, const double* rho_prev, int n
 /* Tile shape and block size the fused path runs with (chosen by the
  * autotuner when jst_opts.tile_i/tile_j are 0); zeros on the passes path. */
 jst_status jst_kernel_config(const jst_solver* s, int* tile_i, int* tile_j, int* block_threads);
+
+/* jst_staging of the fused path's marching strips (0 for tiles and the
+ * passes path).  With JST_STAGING_BULK, a row-copy wait that runs out (about
+ * 0.1 s) makes jst_advance / jst_run return JST_ERR_TIMEOUT. */
+jst_status jst_kernel_staging(const jst_solver* s, int* staging);
 
 /* Version string of this library. */
 const char* jst_version(void);

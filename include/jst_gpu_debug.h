@@ -28,6 +28,12 @@ jst_status jst_debug_set_uniform(jst_solver* s, double rho, double vx, double vy
  * effect on the fused path. */
 jst_status jst_debug_kernel(jst_solver* s, const char* name);
 
+/* Makes every bulk row-copy barrier of the fused path's marching strips
+ * expect `bytes` more than its copies deliver (0 restores it), so that the
+ * kernels' bounded waits run out and the next step returns JST_ERR_TIMEOUT:
+ * the failure path of JST_STAGING_BULK, tested without a fault. */
+jst_status jst_debug_staging_extra_tx(jst_solver* s, int bytes);
+
 /* The fused kernels' FP64 quotient, square root, exponential and inverse
  * sixth root beside CUDA's own, for n operand pairs (a[k], b[k]):
  * out[8k .. 8k+7] = quick a/b, a/b, quick sqrt(b), sqrt(b), quick exp(a),

@@ -20,7 +20,8 @@ from .solver import (DT_LOCAL, OK, PREC_FP32_SPLIT, JstError, NonPhysicalC, lib)
 class BatchOptsC(C.Structure):
     _fields_ = [("precision", C.c_int), ("dt_mode", C.c_int), ("device", C.c_int), ("tile_i", C.c_int),
                 ("tile_j", C.c_int), ("max_instances", C.c_int), ("steps_per_poll", C.c_int),
-                ("hbm_budget_gb", C.c_double), ("keep_fields", C.c_int), ("block_threads", C.c_int)]
+                ("hbm_budget_gb", C.c_double), ("keep_fields", C.c_int), ("block_threads", C.c_int),
+                ("staging", C.c_int)]
 
 
 class BatchResultC(C.Structure):
@@ -55,7 +56,7 @@ class BatchResult:
 # The batch entry points of include/jst_gpu.h this module binds.
 BATCH_EXPORTS = ["jst_batch_default_opts", "jst_batch_create", "jst_batch_destroy", "jst_batch_submit",
                  "jst_batch_step", "jst_batch_stats", "jst_batch_poll", "jst_batch_result_get",
-                 "jst_batch_kernel_config"]
+                 "jst_batch_kernel_config", "jst_batch_kernel_staging"]
 
 
 def _bind():
@@ -71,6 +72,7 @@ def _bind():
     L.jst_batch_step.argtypes = [vp, i]
     L.jst_batch_stats.argtypes = [vp, C.POINTER(i), C.POINTER(i), pd]
     L.jst_batch_kernel_config.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+    L.jst_batch_kernel_staging.argtypes = [vp, C.POINTER(i)]
     L.jst_batch_poll.argtypes = [vp, C.POINTER(C.c_int64), i, C.POINTER(i)]
     L.jst_batch_result_get.argtypes = [vp, C.c_int64, C.POINTER(BatchResultC), pd, C.c_size_t]
     L._batch_bound = True
@@ -79,7 +81,8 @@ def _bind():
 
 class Batch:
     def __init__(self, precision=PREC_FP32_SPLIT, dt_mode=DT_LOCAL, device=0, tile_i=0, tile_j=0,
-                 max_instances=256, steps_per_poll=20, hbm_budget_gb=0.0, keep_fields=False, block_threads=0):
+                 max_instances=256, steps_per_poll=20, hbm_budget_gb=0.0, keep_fields=False, block_threads=0,
+                 staging=0):
         L = _bind()
         o = BatchOptsC()
         L.jst_batch_default_opts(C.byref(o))
@@ -87,6 +90,7 @@ class Batch:
         o.max_instances, o.steps_per_poll, o.hbm_budget_gb = max_instances, steps_per_poll, hbm_budget_gb
         o.keep_fields = 1 if keep_fields else 0
         o.block_threads = block_threads
+        o.staging = staging
         h = C.c_void_p()
         rc = L.jst_batch_create(C.byref(o), C.byref(h))
         if rc != OK:
@@ -133,6 +137,12 @@ class Batch:
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         lib().jst_batch_kernel_config(self._h, C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
+
+    def kernel_staging(self) -> int:
+        """jst_staging of the batch's stage kernel (0 when not marching strips)."""
+        v = C.c_int()
+        lib().jst_batch_kernel_staging(self._h, C.byref(v))
+        return v.value
 
     def poll(self, cap: int = 4096) -> list[int]:
         ids = (C.c_int64 * cap)()

@@ -486,6 +486,8 @@ jst_status jst_advance(jst_solver* s, jst_nonphysical* bad) {
         std::snprintf(buf, sizeof buf, "non-physical state at cell (%lld, %lld): rho = %e, p = %e", (long long)bad->i,
                       (long long)bad->j, bad->rho, bad->p);
         s->err = buf;
+    } else if (rc == JST_ERR_TIMEOUT) {
+        s->err = "a stage kernel's bounded wait for its row copies ran out";
     } else if (rc != JST_OK) {
         s->err = "advance failed";
     }
@@ -509,6 +511,8 @@ jst_status jst_run(jst_solver* s, int64_t max_steps, jst_step_cb cb, void* user,
         std::snprintf(buf, sizeof buf, "non-physical state at cell (%lld, %lld): rho = %e, p = %e", (long long)b->i,
                       (long long)b->j, b->rho, b->p);
         s->err = buf;
+    } else if (rc == JST_ERR_TIMEOUT) {
+        s->err = "a stage kernel's bounded wait for its row copies ran out";
     }
     if (rep) {
         rep->steps = done;
@@ -743,6 +747,12 @@ jst_status jst_kernel_config(const jst_solver* s, int* ti, int* tj, int* nt) {
     return JST_OK;
 }
 
+jst_status jst_kernel_staging(const jst_solver* s, int* staging) {
+    if (!s || !staging) return JST_ERR_ARG;
+    *staging = s->eng->kernel_staging();
+    return JST_OK;
+}
+
 jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_ms) {
     if (!s || !ms || nsteps < 0) return JST_ERR_ARG;
     int64_t before = 0;
@@ -761,6 +771,12 @@ jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_m
 jst_status jst_debug_set_uniform(jst_solver* s, double rho, double vx, double vy, double p, double nut) {
     if (!s) return JST_ERR_ARG;
     s->eng->set_uniform(rho, vx, vy, p, nut);
+    return cudaStreamSynchronize(s->core.st) == cudaSuccess ? JST_OK : JST_ERR_CUDA;
+}
+
+jst_status jst_debug_staging_extra_tx(jst_solver* s, int bytes) {
+    if (!s || bytes < 0 || bytes > (1 << 16)) return JST_ERR_ARG;
+    s->eng->set_stage_extra_tx(bytes);
     return cudaStreamSynchronize(s->core.st) == cudaSuccess ? JST_OK : JST_ERR_CUDA;
 }
 

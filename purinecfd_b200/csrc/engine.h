@@ -76,6 +76,9 @@ class Engine {
         *tj = 0;
         *nt = 0;
     }
+    // jst_staging of the stage kernel (0 when it is not a marching strip)
+    virtual int kernel_staging() const { return 0; }
+    virtual void set_stage_extra_tx(int) {}
     virtual void set_uniform(double, double, double, double, double) {}
     virtual void run_kernel(const char*) {}
 

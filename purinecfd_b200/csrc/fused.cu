@@ -166,6 +166,7 @@ template <class T> struct Kernels {
     size_t smem = 0;
     int nt = 256;
     bool march = false;  // warp per work item (else block per tile)
+    int staging = 0;     // marching strips: 0 per-lane cp.async, 1 bulk (TMA) row copies
 };
 
 template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
@@ -180,17 +181,18 @@ template <class T, int TI, int TJ, int NT> Kernels<T> kernels_for() {
     return k;
 }
 
-template <class T, int NT> Kernels<T> march_kernels_for() {
+template <class T, int NT, int STG = 0> Kernels<T> march_kernels_for() {
     constexpr bool PIPE = true;
     Kernels<T> k;
-    k.stage[0] = fused::k_march<T, NT, true, false, PIPE>;
-    k.stage[1] = fused::k_march<T, NT, false, false, PIPE>;
-    k.stage[2] = fused::k_march<T, NT, false, true, PIPE>;
-    k.dump = fused::k_march<T, NT, true, false, PIPE, true>;
+    k.stage[0] = fused::k_march<T, NT, true, false, PIPE, false, STG>;
+    k.stage[1] = fused::k_march<T, NT, false, false, PIPE, false, STG>;
+    k.stage[2] = fused::k_march<T, NT, false, true, PIPE, false, STG>;
+    k.dump = fused::k_march<T, NT, true, false, PIPE, true, STG>;
     k.step_dt = fused::k_step_dt<T, NT>;
-    k.smem = fused::march_smem_bytes<T, NT, PIPE>();
+    k.smem = fused::march_smem_bytes<T, NT, PIPE, STG>();
     k.nt = NT;
     k.march = true;
+    k.staging = STG;
     return k;
 }
 
@@ -209,7 +211,8 @@ template <class T, int NT> Kernels<T> march2_kernels_for() {
     return k;
 }
 
-template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 256) {
+// staging (marching strips only): 0 per-lane cp.async, 1 bulk row copies
+template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 256, int staging = 0) {
 #define JST_PICK(a, b, n)                               \
     if (ti == a && tj == b && nt == n) {                \
         *out = kernels_for<T, a, b, n>();               \
@@ -219,7 +222,7 @@ template <class T> bool pick_kernels(int ti, int tj, Kernels<T>* out, int nt = 2
 #undef JST_PICK
 #define JST_PICK_MARCH(n)                                           \
     if (ti >= 4 && ti <= 1024 && tj == fused::MARCH_W && nt == n) { \
-        *out = march_kernels_for<T, n>();                           \
+        *out = staging == 1 ? march_kernels_for<T, n, 1>() : march_kernels_for<T, n>(); \
         return true;                                                \
     }
     JST_FOR_MARCH(JST_PICK_MARCH)
@@ -298,6 +301,7 @@ template <class T> __global__ void k_copy_state(Inst<T> I, long n) {
 struct TuneResult {
     int ti, tj, nt;
     float ms;
+    int staging = 0;
 };
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int>, TuneResult> g_tune_cache;
@@ -391,24 +395,27 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    std::vector<std::array<int, 3>> cands;
+    std::vector<std::array<int, 4>> cands;  // (ti, tj, threads, staging)
     const TuneResult m = model_choice<T>(insts);
     if (total_cells(insts) < kTuneMinCells) {
-        for (const auto& cd : kSmallCands) cands.push_back({cd[0], cd[1], cd[2]});
-        cands.push_back({m.ti, m.tj, 64});
+        for (const auto& cd : kSmallCands) cands.push_back({cd[0], cd[1], cd[2], 0});
+        cands.push_back({m.ti, m.tj, 64, 0});
     } else {
-        for (const auto& cd : kTileCands) cands.push_back({cd[0], cd[1], cd[2]});
-        cands.push_back({m.ti, m.tj, 64});
-        cands.push_back({m.ti, m.tj, 128});
+        for (const auto& cd : kTileCands) cands.push_back({cd[0], cd[1], cd[2], 0});
+        cands.push_back({m.ti, m.tj, 64, 0});
+        cands.push_back({m.ti, m.tj, 128, 0});
+        // the same strips with bulk (TMA) row staging
+        cands.push_back({m.ti, m.tj, 64, 1});
+        cands.push_back({m.ti, m.tj, 128, 1});
     }
     if (std::is_same<T, float>::value) {  // paired-column strips
         const TuneResult m2 = model_choice<T>(insts, fused::MARCH2_W);
-        cands.push_back({m2.ti, m2.tj, 64});
-        if (total_cells(insts) >= kTuneMinCells) cands.push_back({m2.ti, m2.tj, 128});
+        cands.push_back({m2.ti, m2.tj, 64, 0});
+        if (total_cells(insts) >= kTuneMinCells) cands.push_back({m2.ti, m2.tj, 128, 0});
     }
     for (const auto& cand : cands) {
         Kernels<T> K;
-        if (!pick_kernels<T>(cand[0], cand[1], &K, cand[2])) continue;
+        if (!pick_kernels<T>(cand[0], cand[1], &K, cand[2], cand[3])) continue;
         if (cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) != cudaSuccess) {
             cudaGetLastError();
             continue;
@@ -444,7 +451,7 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
         }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best.ms) best = TuneResult{cand[0], cand[1], cand[2], ms};
+        if (ms < best.ms) best = TuneResult{cand[0], cand[1], cand[2], ms, cand[3]};
     }
     // undo any NonPhysical flag the timing launches may have raised
     std::vector<InstState> hs(nstates);
@@ -497,8 +504,8 @@ template <class T> class FusedEngine : public Engine {
         if (h_state_) cudaFreeHost(h_state_);
     }
 
-    bool select_kernels(int ti, int tj, int nt, std::string& err) {
-        if (!pick_kernels<T>(ti, tj, &K_, nt)) {
+    bool select_kernels(int ti, int tj, int nt, std::string& err, int staging = 0) {
+        if (!pick_kernels<T>(ti, tj, &K_, nt, staging)) {
             err = "unsupported tile shape " + std::to_string(ti) + "x" + std::to_string(tj) + "x" + std::to_string(nt);
             return false;
         }
@@ -528,7 +535,7 @@ template <class T> class FusedEngine : public Engine {
             default_tile(C.opts.precision, C.nj, &ti, &tj);
             nt = 256;
         }
-        if (!select_kernels(ti, tj, nt, err)) return false;
+        if (!select_kernels(ti, tj, nt, err, C.opts.staging == JST_STAGING_BULK ? 1 : 0)) return false;
         int ni = C.ni, nj = C.nj;
         std::vector<TileRef> tiles = make_tiles(0, ni, nj, ti, tj);
         ntiles_ = (int)tiles.size();
@@ -668,7 +675,9 @@ template <class T> class FusedEngine : public Engine {
             g_tune_cache[key] = r;
         }
         std::string err;
-        if (!select_kernels(r.ti, r.tj, r.nt, err)) return;
+        // a staging the options ask for overrides the tuner's
+        int stg = C.opts.staging == JST_STAGING_BULK ? 1 : (C.opts.staging == JST_STAGING_PER_LANE ? 0 : r.staging);
+        if (!select_kernels(r.ti, r.tj, r.nt, err, stg)) return;
         std::vector<TileRef> tiles = make_tiles(0, C.ni, C.nj, r.ti, r.tj);
         ntiles_ = (int)tiles.size();
         inst_.ntiles = ntiles_;
@@ -685,6 +694,14 @@ template <class T> class FusedEngine : public Engine {
         *ti = ti_;
         *tj = tj_;
         *nt = K_.nt;
+    }
+    int kernel_staging() const override { return K_.march ? (K_.staging == 1 ? JST_STAGING_BULK : JST_STAGING_PER_LANE) : 0; }
+
+    // test hook: bytes the bulk row barrier expects beyond those copied
+    void set_stage_extra_tx(int bytes) override {
+        inst_.stage_extra_tx = bytes;
+        cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, core_->st);
+        cudaStreamSynchronize(core_->st);
     }
 
     void launch_step_dt() {
@@ -753,6 +770,7 @@ template <class T> class FusedEngine : public Engine {
         set_max_step(s.step + 1);
         launch_step();
         if (read_state(&s) != JST_OK) return JST_ERR_CUDA;
+        if (s.err) return JST_ERR_TIMEOUT;
         if (s.bad != fused::NO_BAD) return report(s.bad, bad);
         return JST_OK;
     }
@@ -792,10 +810,11 @@ template <class T> class FusedEngine : public Engine {
                 for (size_t k = 0; k < h.size(); ++k) cb(user, (uint64_t)(reported - start + k + 1), h[k]);
                 reported = s.step;
             }
-            if (s.bad != fused::NO_BAD || s.done || s.step >= start + cap) break;
+            if (s.bad != fused::NO_BAD || s.done || s.err || s.step >= start + cap) break;
         }
         *done = s.step - start;
         *res = s.step > start ? s.residual : std::numeric_limits<double>::quiet_NaN();
+        if (s.err) return JST_ERR_TIMEOUT;
         if (s.bad != fused::NO_BAD) return report(s.bad, bad);
         return JST_OK;
     }
@@ -832,7 +851,7 @@ template <class T> class FusedEngine : public Engine {
                 reported = s.step;
                 cb(user, (uint64_t)(reported - start), s.residual);
             }
-            if (s.bad != fused::NO_BAD || s.done || s.step >= start + cap) break;
+            if (s.bad != fused::NO_BAD || s.done || s.err || s.step >= start + cap) break;
         }
         for (auto& e : ev) cudaEventDestroy(e);
         InstState fin;
@@ -840,6 +859,7 @@ template <class T> class FusedEngine : public Engine {
         if (rc != JST_OK) return rc;
         *done = fin.step - start;
         *res = fin.step > start ? fin.residual : std::numeric_limits<double>::quiet_NaN();
+        if (fin.err) return JST_ERR_TIMEOUT;
         if (fin.bad != fused::NO_BAD) return report(fin.bad, bad);
         return JST_OK;
     }
@@ -1021,6 +1041,7 @@ template <class T> class FusedEngine : public Engine {
         for (auto& e : ev) cudaEventDestroy(e);
         cudaMemcpyAsync(&inst_.st->target, &core_->targetres, sizeof(double), cudaMemcpyHostToDevice, st);
         if (read_state(&s) != JST_OK) return JST_ERR_CUDA;
+        if (s.err) return JST_ERR_TIMEOUT;
         if (s.bad != fused::NO_BAD) return JST_ERR_NONPHYSICAL;
         return JST_OK;
     }
@@ -1120,6 +1141,7 @@ class BatchBase {
     virtual int poll(int64_t* ids, int cap) = 0;
     virtual bool result(int64_t id, BatchResultFull** out) = 0;
     virtual void kernel_config(int* ti, int* tj, int* nt) const = 0;
+    virtual int kernel_staging() const = 0;
 };
 
 template <class T> class Batch : public BatchBase {
@@ -1164,7 +1186,7 @@ template <class T> class Batch : public BatchBase {
             default_tile(o_.precision, 128, &ti, &tj);
             nt = 256;
         }
-        if (!select_kernels(ti, tj, nt)) {
+        if (!select_kernels(ti, tj, nt, o_.staging == JST_STAGING_BULK ? 1 : 0)) {
             err = "unsupported tile shape";
             return false;
         }
@@ -1211,9 +1233,9 @@ template <class T> class Batch : public BatchBase {
         return true;
     }
 
-    bool select_kernels(int ti, int tj, int nt) {
+    bool select_kernels(int ti, int tj, int nt, int staging = 0) {
         Kernels<T> K;
-        if (!pick_kernels<T>(ti, tj, &K, nt)) return false;
+        if (!pick_kernels<T>(ti, tj, &K, nt, staging)) return false;
         for (int k = 0; k < 3; ++k)
             if (cudaFuncSetAttribute(K.stage[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) !=
                 cudaSuccess)
@@ -1243,7 +1265,8 @@ template <class T> class Batch : public BatchBase {
             JST_LAUNCH(k_copy_state<T>, (unsigned)((n + 255) / 256), 256, 0, st_, h_insts_[in.first], n);
         }
         TuneResult r = autotune<T>(list, d_insts_, d_states_, nslots_, st_, 1);
-        if (!select_kernels(r.ti, r.tj, r.nt)) return;
+        const int stg = o_.staging == JST_STAGING_BULK ? 1 : (o_.staging == JST_STAGING_PER_LANE ? 0 : r.staging);
+        if (!select_kernels(r.ti, r.tj, r.nt, stg)) return;
         h_tiles_.clear();
         for (int k = 0; k < nslots_; ++k)
             if (slots_[k].used) {
@@ -1501,6 +1524,11 @@ template <class T> class Batch : public BatchBase {
     jst_status poll_retire() {
         cudaMemcpyAsync(h_states_, d_states_, nslots_ * sizeof(InstState), cudaMemcpyDeviceToHost, st_);
         if (cudaStreamSynchronize(st_) != cudaSuccess) return JST_ERR_CUDA;
+        for (int k = 0; k < nslots_; ++k)
+            if (slots_[k].used && h_states_[k].err) {
+                set_call_error("a stage kernel's bounded wait for its row copies ran out");
+                return JST_ERR_TIMEOUT;
+            }
         std::vector<int> cl_slots;
         for (int k = 0; k < nslots_; ++k)
             if (slots_[k].used && slots_[k].cl_tol > 0.0 && h_states_[k].bad == fused::NO_BAD) {
@@ -1625,6 +1653,7 @@ template <class T> class Batch : public BatchBase {
         *tj = tj_;
         *nt = K_.nt;
     }
+    int kernel_staging() const override { return K_.march ? (K_.staging == 1 ? JST_STAGING_BULK : JST_STAGING_PER_LANE) : 0; }
 
     void stats(int* a, int* q, double* bytes) override {
         if (a) *a = active_;
@@ -1760,6 +1789,12 @@ jst_status jst_batch_step(jst_batch* b, int nsteps) { return b ? b->impl->step(n
 jst_status jst_batch_kernel_config(const jst_batch* b, int* ti, int* tj, int* nt) {
     if (!b || !ti || !tj || !nt) return JST_ERR_ARG;
     b->impl->kernel_config(ti, tj, nt);
+    return JST_OK;
+}
+
+jst_status jst_batch_kernel_staging(const jst_batch* b, int* staging) {
+    if (!b || !staging) return JST_ERR_ARG;
+    *staging = b->impl->kernel_staging();
     return JST_OK;
 }
 

@@ -59,7 +59,7 @@ struct InstState {
     int fresh;         // 1 until the first step completed: stage 0 uses the free-stream primitives
     int done;          // residual fell below target
     int max_step;      // device-side step limit (steps beyond it are skipped)
-    int pad;
+    int err;           // nonzero: a bounded wait in a stage kernel ran out (bulk row staging)
 };
 
 // The per-instance constants of the split precision's marching kernels,
@@ -147,6 +147,9 @@ template <class T> struct Inst {
     // the two columns of each pair interleaved, see k_march_geom2
     const float* mg2;
     ConstP cp;  // make_constp(c)
+    // bulk row staging: bytes the row barrier expects beyond those copied
+    // (0; a test sets it so that the bounded wait runs out)
+    int stage_extra_tx;
     // residual dump (jst_stage_residual): 5 planes of NI*NJ doubles that the
     // DUMP instantiation of stage 0 writes R = Fc - Fv - Fd - S into
     double* rdump;

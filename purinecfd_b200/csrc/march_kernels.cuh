@@ -204,6 +204,73 @@ template <class T> struct MarchRow {
     T volm[32];                       // V of row k-3 (last stage)
 };
 
+// Bulk row staging (STG = 1): the same inputs as MarchRow, but each field's
+// segment of the strip's row is moved by one cp.async.bulk copy (the TMA
+// unit) issued by lane 0, so the buffer mirrors global memory.  A copy must
+// start on a 16-byte boundary and move a multiple of 16 bytes, so a plane of
+// T is staged from the column (j0 - 3) rounded down to a multiple of AT
+// (16 bytes of T) and AT columns wider than the strip; lane L reads column
+// oT + L.  FP64 planes likewise with 2 columns per 16 bytes; the geometry
+// records (32 or 64 bytes each) start exactly at j0 - 3.  A segment that
+// crosses the periodic seam is copied in two pieces.  The copies of a row
+// complete one phase of the row buffer's mbarrier.
+template <class T> struct MarchRowB {
+    static constexpr int AT = 16 / (int)sizeof(T);  // columns of T per 16 bytes
+    static constexpr int WT = 32 + AT;              // columns staged per plane of T
+    static constexpr int WD = 34;                   // columns staged per FP64 plane
+    alignas(16) T rec[32][MG_N];                    // Inst::mg records of row k, one per lane
+    alignas(16) T u[5][WT];                         // stage input of row k
+    alignas(16) T uacc[5][WT];                      // FP32 copy of U_n of row k-3 (split, stages 1-3)
+    alignas(16) double un[5][WD];                   // U_n of row k-3
+    alignas(16) double ldt[WD];                     // dt_local of row k-3
+    alignas(16) double ivm[WD];                     // 1/V of row k-3
+    alignas(16) T rat[WT];                          // V/dt of row k-2 (clamped)
+    alignas(16) T volm[32];                         // V of row k-3 (last stage; per-lane copies)
+    alignas(16) unsigned long long bar;             // the row's mbarrier
+};
+
+#ifdef __CUDA_ARCH__
+JST_D unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+JST_D void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+JST_D void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+JST_D void proxy_async_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// arrive on the barrier and add `bytes` to the transaction count of its phase
+JST_D void mbar_arrive_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// one bulk global -> shared copy (16-byte aligned addresses, size a multiple of 16)
+JST_D void bulk_copy(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+JST_D bool mbar_test(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase of the given parity, at most about `cycles` SM clock
+// cycles; false when the limit ran out.
+JST_D bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, long long cycles) {
+    const long long t0 = clock64();
+    while (!mbar_test(bar, parity))
+        if (clock64() - t0 > cycles) return false;
+    return true;
+}
+#endif
+
+// Limit of a row-buffer wait: about 0.1 s at the B200's SM clock, far beyond
+// any copy's latency.
+constexpr long long kStageWaitCycles = 200000000LL;
+
 // FP64 keeps the 4-row U window in a per-warp shared ring of 5 rows (the
 // registers it would take push the FP64 kernel past 255 registers).
 template <class T> JST_HD constexpr bool march_u_ring() { return sizeof(T) == sizeof(double); }
@@ -217,11 +284,12 @@ template <class T> struct MarchURing {
 // short-latency load instead of a global one (and in FP32 no conversion).
 JST_HD constexpr size_t march_phys_bytes() { return (sizeof(PhysConst) + 15) / 16 * 16; }
 JST_HD constexpr size_t march_const_bytes() { return march_phys_bytes() + (sizeof(ConstP) + 15) / 16 * 16; }
-template <class T, int NT, bool PIPE> JST_HD constexpr size_t march_buf_bytes() {
-    return (size_t)(NT / 32) * ((PIPE ? 2 * sizeof(MarchRow<T>) : 0) + (march_u_ring<T>() ? sizeof(MarchURing<T>) : 0));
+template <class T, int NT, bool PIPE, int STG = 0> JST_HD constexpr size_t march_buf_bytes() {
+    return (size_t)(NT / 32) * ((PIPE ? 2 * (STG ? sizeof(MarchRowB<T>) : sizeof(MarchRow<T>)) : 0) +
+                                (march_u_ring<T>() ? sizeof(MarchURing<T>) : 0));
 }
-template <class T, int NT, bool PIPE> JST_HD constexpr size_t march_smem_bytes() {
-    return march_buf_bytes<T, NT, PIPE>() + (size_t)(NT / 32) * march_const_bytes();
+template <class T, int NT, bool PIPE, int STG = 0> JST_HD constexpr size_t march_smem_bytes() {
+    return march_buf_bytes<T, NT, PIPE, STG>() + (size_t)(NT / 32) * march_const_bytes();
 }
 
 // Copies an instance's constants into this warp's slot (8-byte words, one
@@ -273,12 +341,18 @@ template <class T, int NT> constexpr int march_min_blocks() {
 // sched[0] = number of strips, sched[1] = work counter, sched[2] = exit counter
 // (both zero at launch; the last warp to leave resets them).
 // PIPE: every global input of row k+1 is copied into a per-warp shared
-// buffer (cp.async) while row k is computed, so the walk never waits on HBM
-// latency; without PIPE the loads are issued in the row that uses them.
+// buffer while row k is computed, so the walk never waits on HBM latency;
+// without PIPE the loads are issued in the row that uses them.  STG selects
+// how the copies are made: 0, one cp.async per lane and field; 1, one
+// cp.async.bulk (TMA) copy per field's row segment issued by lane 0 and
+// completed on the row buffer's mbarrier (MarchRowB), where the ring allows
+// it (NJ a multiple of 16 bytes of T and at least 36 columns), else per-lane
+// copies into the same layout.  A bounded wait that runs out sets
+// InstState::err, and the warp does no further work in the launch.
 // DUMP (with FIRST only): the residual R of every cell of the current state
 // goes to Inst::rdump instead of an update; nothing else is written and the
 // instance's step counters and stop flags are ignored.
-template <class T, int NT, bool FIRST, bool LAST, bool PIPE = false, bool DUMP = false>
+template <class T, int NT, bool FIRST, bool LAST, bool PIPE = false, bool DUMP = false, int STG = 0>
 __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage,
                                               double alpha) {
     using TD = typename std::conditional<LAST, double, T>::type;
@@ -289,20 +363,33 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
     // from rounding U_n - increment once by at most one FP32 rounding); the
     // last stage adds its increment to U_n in FP64.
     constexpr bool ACC32 = sizeof(T) == sizeof(float) && !LAST;
-    MarchRow<T>* rowbuf = nullptr;
+    using RowT = typename std::conditional<STG == 1, MarchRowB<T>, MarchRow<T>>::type;
+    RowT* rowbuf = nullptr;
     MarchURing<T>* uring = nullptr;
     JST_DYN_SMEM(smem_raw);
     const int wib = JST_WARP_IN_BLOCK();
-    if constexpr (PIPE) rowbuf = reinterpret_cast<MarchRow<T>*>(smem_raw) + 2 * wib;
+    if constexpr (PIPE) rowbuf = reinterpret_cast<RowT*>(smem_raw) + 2 * wib;
     if constexpr (UR)
-        uring = reinterpret_cast<MarchURing<T>*>(smem_raw + (PIPE ? (size_t)(NT / 32) * 2 * sizeof(MarchRow<T>) : 0)) + wib;
-    PhysConst* cwarp =
-        reinterpret_cast<PhysConst*>(smem_raw + march_buf_bytes<T, NT, PIPE>() + (size_t)wib * march_const_bytes());
+        uring = reinterpret_cast<MarchURing<T>*>(smem_raw + (PIPE ? (size_t)(NT / 32) * 2 * sizeof(RowT) : 0)) + wib;
+    PhysConst* cwarp = reinterpret_cast<PhysConst*>(smem_raw + march_buf_bytes<T, NT, PIPE, STG>() +
+                                                    (size_t)wib * march_const_bytes());
     ConstP* kwarp = reinterpret_cast<ConstP*>(reinterpret_cast<unsigned char*>(cwarp) + march_phys_bytes());
     const int nt_all = sched[0];
     unsigned* work = reinterpret_cast<unsigned*>(sched + 1);
     unsigned* exitc = reinterpret_cast<unsigned*>(sched + 2);
     const unsigned nwarps = (unsigned)JST_GRID() * (NT / 32);
+    unsigned bphase = 0;  // STG 1: parity of the next phase of each row buffer's barrier (bit b)
+    bool dead = false;    // STG 1: a bounded wait ran out; take no more work
+#ifdef __CUDA_ARCH__
+    if constexpr (STG == 1) {
+        if (lane == 0) {
+            mbar_init(&rowbuf[0].bar);
+            mbar_init(&rowbuf[1].bar);
+            mbar_init_fence();
+        }
+        __syncwarp();
+    }
+#endif
     for (;;) {
         unsigned ticket = 0;
         if (lane == 0) ticket = atomicAdd(work, 1u);
@@ -314,6 +401,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             }
             break;
         }
+        if (dead) continue;
         const TileRef tr = tiles[ticket];
         const Inst<T>& I = insts[tr.inst];
         const int ni = I.ni, nj = I.nj, i0 = tr.i0, j0 = tr.j0;
@@ -365,19 +453,88 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         // so the pressure reference of euler_flux is doubled as well
         const T p_ref2 = sizeof(T) == sizeof(double) ? T(0) : kc<T>(0.0, K.p_ref2);
 
+        // STG 1: bulk copies where the ring allows them (16-byte aligned
+        // segments; a segment crosses the seam at most once); the columns
+        // oT, oD of the staged segments hold the strip's first column
+        constexpr int AT = MarchRowB<T>::AT, WT = MarchRowB<T>::WT, WD = MarchRowB<T>::WD;
+        const bool bulk = STG == 1 && nj % AT == 0 && nj >= WT;
+        const int sT = (j0 - 3) & ~(AT - 1), sD = (j0 - 3) & ~1;
+        const int oT = bulk ? j0 - 3 - sT : 0, oD = bulk ? j0 - 3 - sD : 0;
+        const unsigned extra_tx = STG == 1 ? (unsigned)I.stage_extra_tx : 0u;
+        bool failed = false;
+        (void)sD;
+        (void)extra_tx;
+
         // PIPE: stage the global inputs that row kk of the walk reads.  The
         // conditions are the ones under which the walk reads them.
+        auto issue_bulk = [&](auto steady, int kk) {
+            constexpr bool S = decltype(steady)::value;
+            RowT& B = rowbuf[kk & 1];
+#ifdef __CUDA_ARCH__
+            if constexpr (STG == 1) {
+                __syncwarp();  // every lane has read this buffer's previous row
+                if (lane == 0) {
+                    unsigned tx = 0;
+                    // columns c0 .. c0+w-1 of a row (elements of esz bytes), wrapped
+                    auto seg = [&](void* d, const void* rowp, int esz, int c0, int w) {
+                        const int a = c0 < 0 ? c0 + nj : c0;
+                        const int n1 = w < nj - a ? w : nj - a;
+                        bulk_copy(d, static_cast<const char*>(rowp) + (long)a * esz, (unsigned)(n1 * esz), &B.bar);
+                        if (n1 < w)
+                            bulk_copy(static_cast<char*>(d) + (long)n1 * esz, rowp, (unsigned)((w - n1) * esz), &B.bar);
+                        tx += (unsigned)(w * esz);
+                    };
+                    if (S || kk < ni) {
+                        const long row = kk < 0 ? -1 - kk : kk;
+                        for (int v = 0; v < 5; ++v) seg(B.u[v], src + v * np + row * nj, (int)sizeof(T), sT, WT);
+                    }
+                    if (S || (kk >= 0 && kk <= ni))
+                        seg(B.rec, I.mg + MG_N * ((long)kk * nj), MG_N * (int)sizeof(T), j0 - 3, 32);
+                    const int rr = kk - 2;
+                    if (S || (rr >= i0 - 1 && rr <= i1)) {
+                        const int gc = S ? rr : (rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr));
+                        seg(B.rat, ratio + (long)gc * nj, (int)sizeof(T), sT, WT);
+                    }
+                    const int m = kk - 3;
+                    if (S || (m >= i0 && m < i1)) {
+                        const long mr = (long)m * nj;
+                        if constexpr (ACC32) {
+                            if constexpr (!FIRST)
+                                for (int v = 0; v < 5; ++v) seg(B.uacc[v], I.uc[0] + v * np + mr, (int)sizeof(T), sT, WT);
+                        } else {
+                            for (int v = 0; v < 5; ++v) seg(B.un[v], I.un[0] + v * np + mr, 8, sD, WD);
+                        }
+                        if (dt_local) seg(B.ldt, I.ldt + mr, 8, sD, WD);
+                        seg(B.ivm, I.inv_vol + mr, 8, sD, WD);
+                    }
+                    mbar_arrive_tx(&B.bar, tx + extra_tx);
+                }
+                const int m = kk - 3;
+                if (LAST && (S || (m >= i0 && m < i1)))
+                    async_copy<sizeof(T)>(&B.volm[lane], I.mg + MG_N * ((long)(m + 1) * nj + gj) + MG_VOL);
+            }
+#endif
+            (void)B;
+            (void)kk;
+        };
         auto issue = [&](auto steady, int kk) {
             constexpr bool S = decltype(steady)::value;  // kk is a steady row
-            MarchRow<T>& B = rowbuf[kk & 1];
+            if (STG == 1 && bulk) {
+                issue_bulk(steady, kk);
+                return;
+            }
+            RowT& B = rowbuf[kk & 1];
+            auto rec_dst = [&](int ch) -> T* {
+                if constexpr (STG == 1) return &B.rec[lane][ch * MarchRow<T>::EPC];
+                else return &B.rec[ch][lane][0];
+            };
             if (S || kk < ni) {
                 const long id = (long)(kk < 0 ? -1 - kk : kk) * nj + gj;
                 for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.u[v][lane], src + v * np + id);
             }
             if (S || (kk >= 0 && kk <= ni)) {
                 const T* g = I.mg + MG_N * ((long)kk * nj + gj);
-                for (int ch = 0; ch < MarchRow<T>::RCH; ++ch)
-                    async_copy<16>(&B.rec[ch][lane][0], g + ch * MarchRow<T>::EPC);
+                for (int ch = 0; ch < MarchRow<T>::RCH; ++ch) async_copy<16>(rec_dst(ch), g + ch * MarchRow<T>::EPC);
             }
             const int rr = kk - 2;
             if (S || (rr >= i0 - 1 && rr <= i1)) {
@@ -438,7 +595,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         // too, so the range tests drop out and the body is one straight block.
         auto row = [&](auto steady, int k) {
             constexpr bool S = decltype(steady)::value;
-            const MarchRow<T>* B = nullptr;
+            const RowT* B = nullptr;
             // U of row k-4+a (a = 0..3): the register window, or the ring slot
             const int s0 = UR ? ((k % 5) + 5) % 5 : 0;  // ring slot of row k
             auto UA = [&](int a, int v) -> T {
@@ -455,6 +612,21 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 async_commit();
                 async_wait_prior1();
                 B = &rowbuf[k & 1];
+#ifdef __CUDA_ARCH__
+                if constexpr (STG == 1) if (bulk) {
+                    const unsigned b = (unsigned)(k & 1);
+                    const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&rowbuf[b].bar, (bphase >> b) & 1u,
+                                                                              kStageWaitCycles));
+                    bphase ^= 1u << b;
+                    if (!ok) {  // record it, let the copies in flight land, stop
+                        if (lane == 0) atomicOr(&I.st->err, 1);
+                        __all_sync(0xffffffffu, mbar_wait_bounded(&rowbuf[b ^ 1u].bar, (bphase >> (b ^ 1u)) & 1u,
+                                                                  kStageWaitCycles));
+                        failed = true;
+                        return;
+                    }
+                }
+#endif
             }
             // ---- row k: conserved state and primitives ---------------------
             T uk[5], pk, qk[4];
@@ -462,7 +634,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                 const bool wall = !S && k < 0;
                 const int kr = wall ? -1 - k : k;  // the wall ghost mirrors cell -1-k (boundary.rs:30-51)
                 const long id = (long)kr * nj + gj;
-                for (int v = 0; v < 5; ++v) uk[v] = PIPE ? B->u[v][lane] : ld(src + v * np + id);
+                for (int v = 0; v < 5; ++v) uk[v] = PIPE ? B->u[v][oT + lane] : ld(src + v * np + id);
                 Prim<T> p;
                 if (fresh) {
                     p.rho = kc<T>(c.f_rho, K.f_rho);
@@ -531,7 +703,10 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             if (S || (k >= 0 && k <= ni)) {
                 if constexpr (PIPE) {
                     for (int ch = 0; ch < MarchRow<T>::RCH; ++ch)
-                        for (int e = 0; e < MarchRow<T>::EPC; ++e) gk[ch * MarchRow<T>::EPC + e] = B->rec[ch][lane][e];
+                        for (int e = 0; e < MarchRow<T>::EPC; ++e) {
+                            if constexpr (STG == 1) gk[ch * MarchRow<T>::EPC + e] = B->rec[lane][ch * MarchRow<T>::EPC + e];
+                            else gk[ch * MarchRow<T>::EPC + e] = B->rec[ch][lane][e];
+                        }
                 } else {
                     const T* g = I.mg + MG_N * ((long)k * nj + gj);
                     for (int e = 0; e < MG_N; ++e) gk[e] = ld(g + e);
@@ -614,7 +789,7 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             {
                 int rr = k - 2;
                 int gc = S ? rr : (rr < 0 ? 0 : (rr > ni - 1 ? ni - 1 : rr));
-                if (S || (rr >= i0 - 1 && rr <= i1)) rtn = PIPE ? B->rat[lane] : ld(ratio + (long)gc * nj + gj);
+                if (S || (rr >= i0 - 1 && rr <= i1)) rtn = PIPE ? B->rat[oT + lane] : ld(ratio + (long)gc * nj + gj);
             }
 
             // ---- tau face f = k-2 (between rows k-3 and k-2) ---------------
@@ -691,17 +866,17 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
                     T R[5];
                     for (int v = 0; v < 5; ++v) R[v] = (ftn[v] - ft[v]) + (fnr[v] - fn[v]);
                     R[4] -= sw[0];
-                    double a = dt_local ? alpha * (PIPE ? B->ldt[lane] : ld(I.ldt + id)) : adt;
-                    double sc = a * (PIPE ? B->ivm[lane] : ld(I.inv_vol + id));
+                    double a = dt_local ? alpha * (PIPE ? B->ldt[oD + lane] : ld(I.ldt + id)) : adt;
+                    double sc = a * (PIPE ? B->ivm[oD + lane] : ld(I.inv_vol + id));
                     double un[5], uo0 = 0.0;
                     for (int v = 0; v < 5; ++v) {
                         if constexpr (ACC32) {
-                            T a0 = FIRST ? UA(1, v) : (PIPE ? B->uacc[v][lane] : ld(I.uc[0] + v * np + id));
+                            T a0 = FIRST ? UA(1, v) : (PIPE ? B->uacc[v][oT + lane] : ld(I.uc[0] + v * np + id));
                             T nv = a0 - R[v] * (T)sc;
                             un[v] = (double)nv;
                             if (out_lane) dst[v * np + id] = (TD)nv;
                         } else {
-                            double uo = PIPE ? B->un[v][lane] : I.un[0][v * np + id];
+                            double uo = PIPE ? B->un[v][oD + lane] : I.un[0][v * np + id];
                             if (v == 0) uo0 = uo;
                             if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
                             else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
@@ -800,14 +975,18 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             // out of line (its captured windows then pass through the
             // stack); a single call site keeps it inline.
             for (int ph = 0; ph < 2; ++ph) {
-                for (; k <= (ph == 0 ? ks0 - 1 : i1 + 2) && k <= i1 + 2; ++k) row(std::false_type{}, k);
+                for (; k <= (ph == 0 ? ks0 - 1 : i1 + 2) && k <= i1 + 2 && !failed; ++k) row(std::false_type{}, k);
                 if (ph == 0)
-                    for (; k <= ks1; ++k) row(std::true_type{}, k);
+                    for (; k <= ks1 && !failed; ++k) row(std::true_type{}, k);
             }
         } else {
-            for (; k < ks0 && k <= i1 + 2; ++k) row(std::false_type{}, k);
-            for (; k <= ks1; ++k) row(std::true_type{}, k);
-            for (; k <= i1 + 2; ++k) row(std::false_type{}, k);
+            for (; k < ks0 && k <= i1 + 2 && !failed; ++k) row(std::false_type{}, k);
+            for (; k <= ks1 && !failed; ++k) row(std::true_type{}, k);
+            for (; k <= i1 + 2 && !failed; ++k) row(std::false_type{}, k);
+        }
+        if (failed) {  // the strip is abandoned (InstState::err is set)
+            dead = true;
+            continue;
         }
 
         if (LAST) {

@@ -31,6 +31,7 @@ STATUS_NAMES = ["OK", "MESH_IO", "MESH_BAD_HEADER", "MESH_EMPTY", "MESH_COUNT_MI
 PREC_FP64, PREC_FP32_SPLIT = 0, 1
 DT_GLOBAL, DT_LOCAL = 0, 1
 PATH_FUSED, PATH_PASSES = 0, 1
+STAGING_AUTO, STAGING_PER_LANE, STAGING_BULK = 0, 1, 2
 
 FIELDS = (["rho", "p", "T", "u", "v", "E", "H", "c", "nut"] + [f"U{k}" for k in range(5)] +
           [f"Fc{k}" for k in range(5)] + [f"Fv{k}" for k in range(5)] + [f"Fd{k}" for k in range(5)] +
@@ -43,15 +44,15 @@ EXPORTS = ["jst_default_opts", "jst_create_from_paths", "jst_create", "jst_destr
            "jst_nj", "jst_advance", "jst_run", "jst_residual_terms", "jst_timestep", "jst_residual",
            "jst_totaltime", "jst_step_count", "jst_get_field", "jst_get_faces", "jst_set_conserved",
            "jst_forces", "jst_write_csv", "jst_version", "jst_time_steps", "jst_residual_noalloc", "jst_kernel_config",
-           "jst_checkpoint_save", "jst_checkpoint_load", "jst_stage_residual"]
+           "jst_checkpoint_save", "jst_checkpoint_load", "jst_stage_residual", "jst_kernel_staging"]
 # test hooks declared in include/jst_gpu_debug.h
-DEBUG_EXPORTS = ["jst_debug_set_uniform", "jst_debug_kernel", "jst_debug_quick_arith"]
+DEBUG_EXPORTS = ["jst_debug_set_uniform", "jst_debug_kernel", "jst_debug_quick_arith", "jst_debug_staging_extra_tx"]
 
 
 class Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("dt_mode", C.c_int), ("kernel_path", C.c_int), ("device", C.c_int),
                 ("tile_i", C.c_int), ("tile_j", C.c_int), ("use_graph", C.c_int), ("nut_inf_ratio", C.c_double),
-                ("block_threads", C.c_int)]
+                ("block_threads", C.c_int), ("staging", C.c_int)]
 
 
 class NonPhysicalC(C.Structure):
@@ -127,6 +128,8 @@ def lib() -> C.CDLL:
         L.jst_time_steps.argtypes = [vp, i, pd, pd]
         L.jst_residual_noalloc.argtypes = [vp, vp, i, i, vp, vp]
         L.jst_kernel_config.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+        L.jst_kernel_staging.argtypes = [vp, C.POINTER(i)]
+        L.jst_debug_staging_extra_tx.argtypes = [vp, i]
         L.jst_debug_set_uniform.argtypes = [vp, d, d, d, d, d]
         L.jst_debug_kernel.argtypes = [vp, C.c_char_p]
         L.jst_debug_quick_arith.argtypes = [pd, pd, pd, sz]
@@ -139,12 +142,13 @@ def _ptr(a: np.ndarray):
 
 
 def make_opts(precision=PREC_FP64, dt_mode=DT_GLOBAL, kernel_path=PATH_FUSED, device=0, tile_i=0, tile_j=0,
-              use_graph=1, nut_inf_ratio=0.0, block_threads=0) -> Opts:
+              use_graph=1, nut_inf_ratio=0.0, block_threads=0, staging=0) -> Opts:
     o = Opts()
     lib().jst_default_opts(C.byref(o))
     o.precision, o.dt_mode, o.kernel_path, o.device = precision, dt_mode, kernel_path, device
     o.tile_i, o.tile_j, o.use_graph, o.nut_inf_ratio = tile_i, tile_j, use_graph, nut_inf_ratio
     o.block_threads = block_threads
+    o.staging = staging
     return o
 
 
@@ -313,7 +317,18 @@ class Solver:
         self._check(lib().jst_kernel_config(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
 
+    def kernel_staging(self) -> int:
+        """STAGING_PER_LANE or STAGING_BULK for marching strips, 0 otherwise."""
+        v = C.c_int()
+        self._check(lib().jst_kernel_staging(self._h, C.byref(v)))
+        return v.value
+
     # test hooks
+    def debug_staging_extra_tx(self, nbytes: int):
+        """Make every bulk row-copy barrier expect nbytes more than its copies
+        deliver (0 restores it): the bounded waits run out."""
+        self._check(lib().jst_debug_staging_extra_tx(self._h, int(nbytes)))
+
     def set_uniform(self, rho, vx, vy, p, nut):
         self._check(lib().jst_debug_set_uniform(self._h, rho, vx, vy, p, nut))
 

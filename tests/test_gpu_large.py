@@ -56,12 +56,23 @@ def naca_4097():
     return cfg, xy, nr, nt, hist, fields, resid
 
 
-@pytest.mark.parametrize("kernel", ["autotuned", "strips_47x26x64", "strips_94x26x128"])
+def _kernel_opts(kernel: str) -> dict:
+    """Solver options of a kernel label: autotuned, strips_HxWxT (per-lane
+    staging), bulk_HxWxT (bulk row staging), pairs_HxWxT."""
+    if kernel == "autotuned":
+        return {}
+    h, w, t = map(int, kernel.split("_")[1].split("x"))
+    kw = dict(tile_i=h, tile_j=w, block_threads=t)
+    if kernel.startswith("bulk"):
+        kw["staging"] = 2
+    return kw
+
+
+@pytest.mark.parametrize("kernel", ["autotuned", "strips_47x26x64", "strips_94x26x128", "bulk_47x26x64"])
 def test_benchmark_mesh_fp64_matches_oracle(naca_4097, kernel):
     from purinecfd_b200 import PREC_FP64, Solver
     cfg, xy, nr, nt, hist_o, fields_o, resid_o = naca_4097
-    kw = {} if kernel == "autotuned" else dict(tile_i=int(kernel.split("_")[1].split("x")[0]), tile_j=26,
-                                                block_threads=int(kernel.split("x")[-1]))
+    kw = _kernel_opts(kernel)
     s = Solver(cfg, xy, nr, nt, precision=PREC_FP64, **kw)
     hist = []
     rep = s.run(STEPS, lambda k, r: hist.append(r))
@@ -76,13 +87,11 @@ def test_benchmark_mesh_fp64_matches_oracle(naca_4097, kernel):
     s.close()
 
 
-@pytest.mark.parametrize("kernel", ["autotuned", "strips_94x26x128", "pairs_64x56x64"])
+@pytest.mark.parametrize("kernel", ["autotuned", "strips_94x26x128", "bulk_94x26x128", "pairs_64x56x64"])
 def test_benchmark_mesh_split_within_tolerance(naca_4097, kernel):
     from purinecfd_b200 import PREC_FP32_SPLIT, Solver
     cfg, xy, nr, nt, hist_o, fields_o, _ = naca_4097
-    kw = {} if kernel == "autotuned" else dict(tile_i=int(kernel.split("_")[1].split("x")[0]),
-                                                tile_j=int(kernel.split("x")[1]),
-                                                block_threads=int(kernel.split("x")[-1]))
+    kw = _kernel_opts(kernel)
     s = Solver(cfg, xy, nr, nt, precision=PREC_FP32_SPLIT, **kw)
     rep = s.run(STEPS)
     assert rep.steps == STEPS
