@@ -73,10 +73,14 @@ template <class T> JST_HD T powi6(T x) {
 // Both stay within one unit in the last place of the correctly rounded
 // result for normal finite operands (b != 0, x > 0), which is all these
 // kernels divide by or take roots of; a NaN operand gives NaN.  In float the
-// translation unit's division and root are used as they are.
+// quotient is the hardware's approximate division (__fdividef: the
+// reciprocal approximation times a, within 2 units in the last place for
+// |b| < 2^126, beyond every quantity these kernels divide by), and the root
+// the translation unit's square root.
 template <class T, bool Q = false> JST_HD T dv(T a, T b) { return a / b; }
 template <class T, bool Q = false> JST_HD T sq(T x) { return sqrt(x); }
 #ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ float dv<float, true>(float a, float b) { return __fdividef(a, b); }
 template <> __device__ __forceinline__ double dv<double, true>(double a, double b) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
@@ -347,7 +351,7 @@ JST_HD float fw_f32(float r, float cw2, float cw3_6, float one_plus_cw3_6, float
     const float rc = fmaxf(r, -1e4f);
     const float g = rc + cw2 * (powi6<float>(rc) - rc);
     const float gf = fminf(g, 1e5f);  // NaN passes through
-    const float v = gf * root6_f32(one_plus_cw3_6 / (powi6<float>(gf) + cw3_6));
+    const float v = gf * root6_f32(dv<float, true>(one_plus_cw3_6, powi6<float>(gf) + cw3_6));
     return g > 1e5f ? fw_lim : v;
 }
 

@@ -315,14 +315,14 @@ template <class T> JST_D T kc(double d, float2 f) {
 // source::compute for one cell in FP32 (sa_source) from the FP32 constants.
 JST_D float sa_source_f32(float rho, float rho_nu, float inv_dist2, float chi, float f1, float dvdx, float dudy,
                           float dnx, float dny, const ConstP& K) {
-    const float nu_tilde = rho_nu / rho;
+    const float nu_tilde = dv<float, true>(rho_nu, rho);
     const float inv_kd2 = inv_dist2 * K.inv_kappa2.x;
     const float ft2 = K.ct3.x * exp_f32(K.m_ct4.x * chi * chi);
-    const float fv2 = 1.0f - chi / (1.0f + chi * f1);
+    const float fv2 = 1.0f - dv<float, true>(chi, 1.0f + chi * f1);
     const float sv = K.fv3.x * fabsf(dvdx - dudy);
     const float s_tilde = fmaxf(sv + nu_tilde * inv_kd2 * fv2, 1e-10f);
     const float prod = K.cb1.x * (1.0f - ft2) * s_tilde * rho_nu;
-    const float r = fminf(nu_tilde / s_tilde * inv_kd2, K.rmax.x);
+    const float r = fminf(dv<float, true>(nu_tilde, s_tilde) * inv_kd2, K.rmax.x);
     const float fw = fw_f32(r, K.cw2.x, K.cw3_6.x, K.one_plus_cw3_6.x, K.fw_lim.x);
     const float destr = (K.cw1.x * fw + K.m_cb1_k2.x * ft2) * rho * (nu_tilde * nu_tilde * inv_dist2);
     const float diff = K.cb2_sigma.x * rho * (dnx * dnx + dny * dny);
