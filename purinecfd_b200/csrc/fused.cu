@@ -163,6 +163,9 @@ template <class T> struct Kernels {
     void (*step_dt)(const TileRef*, const int*, const Inst<T>*, int, int) = nullptr;
     // stage 0 writing the residual of every cell to Inst::rdump (jst_stage_residual)
     void (*dump)(const TileRef*, int*, const Inst<T>*, int, double) = nullptr;
+    // single-instance marching strips (per-lane staging): the same stages with
+    // the instance descriptor passed by value (k_march_solo)
+    void (*solo[3])(const TileRef*, int*, int, double, Inst<T>) = {nullptr, nullptr, nullptr};
     size_t smem = 0;
     int nt = 256;
     bool march = false;  // warp per work item (else block per tile)
@@ -188,6 +191,11 @@ template <class T, int NT, int STG = 0> Kernels<T> march_kernels_for() {
     k.stage[1] = fused::k_march<T, NT, false, false, PIPE, false, STG>;
     k.stage[2] = fused::k_march<T, NT, false, true, PIPE, false, STG>;
     k.dump = fused::k_march<T, NT, true, false, PIPE, true, STG>;
+    if constexpr (STG == 0) {
+        k.solo[0] = fused::k_march_solo<T, NT, true, false>;
+        k.solo[1] = fused::k_march_solo<T, NT, false, false>;
+        k.solo[2] = fused::k_march_solo<T, NT, false, true>;
+    }
     k.step_dt = fused::k_step_dt<T, NT>;
     k.smem = fused::march_smem_bytes<T, NT, PIPE, STG>();
     k.nt = NT;
@@ -384,7 +392,7 @@ long total_cells(const std::vector<std::pair<int, std::pair<int, int>>>& insts) 
 // (their U_a must hold a valid state) and returns the fastest configuration.
 template <class T>
 TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& insts, Inst<T>* d_insts,
-                    InstState* d_states, int nstates, cudaStream_t st, int grid_hint) {
+                    InstState* d_states, int nstates, cudaStream_t st, int grid_hint, const Inst<T>* h_solo = nullptr) {
     TuneResult best{8, 32, 256, 1e30f};
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -416,7 +424,10 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
     for (const auto& cand : cands) {
         Kernels<T> K;
         if (!pick_kernels<T>(cand[0], cand[1], &K, cand[2], cand[3])) continue;
-        if (cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) != cudaSuccess) {
+        const bool solo = h_solo && K.solo[1];  // time the kernel a single solve runs
+        if (cudaFuncSetAttribute(K.stage[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) != cudaSuccess ||
+            (solo && cudaFuncSetAttribute(K.solo[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem) !=
+                         cudaSuccess)) {
             cudaGetLastError();
             continue;
         }
@@ -441,9 +452,13 @@ TuneResult autotune(const std::vector<std::pair<int, std::pair<int, int>>>& inst
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K.stage[1], K.nt, K.smem);
         int grid = K.march ? stage_grid(K, nt_, sms * std::max(1, occ))
                            : (grid_hint > 0 ? std::min(nt_, sms * std::max(1, occ)) : nt_);
-        JST_LAUNCH(K.stage[1], grid, K.nt, K.smem, st, d_t, d_n, d_insts, 1, RK_ALPHA[1]);  // warm-up
+        auto launch = [&]() {
+            if (solo) JST_LAUNCH(K.solo[1], grid, K.nt, K.smem, st, d_t, d_n, 1, RK_ALPHA[1], *h_solo);
+            else JST_LAUNCH(K.stage[1], grid, K.nt, K.smem, st, d_t, d_n, d_insts, 1, RK_ALPHA[1]);
+        };
+        launch();  // warm-up
         cudaEventRecord(e0, st);
-        for (int r = 0; r < 3; ++r) JST_LAUNCH(K.stage[1], grid, K.nt, K.smem, st, d_t, d_n, d_insts, 1, RK_ALPHA[1]);
+        for (int r = 0; r < 3; ++r) launch();
         cudaEventRecord(e1, st);
         if (cudaEventSynchronize(e1) != cudaSuccess) {
             cudaGetLastError();
@@ -511,7 +526,10 @@ template <class T> class FusedEngine : public Engine {
         }
         for (int k = 0; k < 4; ++k)
             if (cudaFuncSetAttribute(k < 3 ? K_.stage[k] : K_.dump, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)K_.smem) != cudaSuccess) {
+                                     (int)K_.smem) != cudaSuccess ||
+                (k < 3 && K_.solo[k] &&
+                 cudaFuncSetAttribute(K_.solo[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K_.smem) !=
+                     cudaSuccess)) {
                 err = "stage kernel needs " + std::to_string(K_.smem) + " bytes of shared memory";
                 return false;
             }
@@ -609,7 +627,7 @@ template <class T> class FusedEngine : public Engine {
         d_field_ = reinterpret_cast<double*>(base + o_field);
         inst_.mg = reinterpret_cast<T*>(base + o_mg);
         inst_.mg2 = march2_geom_bytes<T>(ni, nj) ? reinterpret_cast<float*>(base + o_mg2) : nullptr;
-        cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
+        upload_inst(C.st);
         cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_ntiles_, &ntiles_, sizeof(int), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_unptr_, inst_.un, 5 * sizeof(double*), cudaMemcpyHostToDevice, C.st);
@@ -670,7 +688,7 @@ template <class T> class FusedEngine : public Engine {
         if (!have) {
             long n = (long)C.ni * C.nj;
             JST_LAUNCH(k_copy_state<T>, (unsigned)((n + 255) / 256), 256, 0, C.st, inst_, n);
-            r = autotune<T>({{0, {C.ni, C.nj}}}, d_inst_, inst_.st, 1, C.st, 0);
+            r = autotune<T>({{0, {C.ni, C.nj}}}, d_inst_, inst_.st, 1, C.st, 0, &inst_);
             std::lock_guard<std::mutex> lock(g_tune_mu);
             g_tune_cache[key] = r;
         }
@@ -681,7 +699,7 @@ template <class T> class FusedEngine : public Engine {
         std::vector<TileRef> tiles = make_tiles(0, C.ni, C.nj, r.ti, r.tj);
         ntiles_ = (int)tiles.size();
         inst_.ntiles = ntiles_;
-        cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
+        upload_inst(C.st);
         cudaMemcpyAsync(d_tiles_, tiles.data(), tiles.size() * sizeof(TileRef), cudaMemcpyHostToDevice, C.st);
         cudaMemcpyAsync(d_ntiles_, &ntiles_, sizeof(int), cudaMemcpyHostToDevice, C.st);
         reset_state(1);
@@ -700,7 +718,7 @@ template <class T> class FusedEngine : public Engine {
     // test hook: bytes the bulk row barrier expects beyond those copied
     void set_stage_extra_tx(int bytes) override {
         inst_.stage_extra_tx = bytes;
-        cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, core_->st);
+        upload_inst(core_->st);
         cudaStreamSynchronize(core_->st);
     }
 
@@ -708,10 +726,27 @@ template <class T> class FusedEngine : public Engine {
         JST_LAUNCH(K_.step_dt, ntiles_, K_.nt, 0, core_->st, d_tiles_, d_ntiles_, d_inst_, ti_, tj_);
     }
 
+    // RK stage s (0..4); the marching strips take the instance descriptor by
+    // value (a captured graph holds the value, so every change of inst_
+    // goes through upload_inst, which drops the graph)
+    void launch_stage(int s, cudaStream_t st) {
+        const int k = s == 0 ? 0 : (s == 4 ? 2 : 1);
+        if (K_.solo[k]) JST_LAUNCH(K_.solo[k], sgrid(), K_.nt, K_.smem, st, d_tiles_, d_ntiles_, s, RK_ALPHA[s], inst_);
+        else JST_LAUNCH(K_.stage[k], sgrid(), K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, s, RK_ALPHA[s]);
+    }
+
     void enqueue_step(cudaStream_t st) {
-        for (int s = 0; s < 5; ++s) {
-            auto kern = s == 0 ? K_.stage[0] : (s == 4 ? K_.stage[2] : K_.stage[1]);
-            JST_LAUNCH(kern, sgrid(), K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, s, RK_ALPHA[s]);
+        for (int s = 0; s < 5; ++s) launch_stage(s, st);
+    }
+
+    // Copies inst_ to the device (stream-ordered) and drops the captured step
+    // graph, whose solo launches hold the previous value.
+    void upload_inst(cudaStream_t st) {
+        cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, st);
+        if (graph_exec_) {
+            cudaStreamSynchronize(st);
+            cudaGraphExecDestroy(graph_exec_);
+            graph_exec_ = nullptr;
         }
     }
 
@@ -874,7 +909,7 @@ template <class T> class FusedEngine : public Engine {
         extra_hist_ = h;
         inst_.res_hist = h;
         hist_cap_ = cap;
-        cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, core_->st);
+        upload_inst(core_->st);
         cudaStreamSynchronize(core_->st);
     }
 
@@ -894,7 +929,7 @@ template <class T> class FusedEngine : public Engine {
         if (!rdump_) {
             if (cudaMalloc(&rdump_, 5 * n * sizeof(double)) != cudaSuccess) return JST_ERR_OOM;
             inst_.rdump = rdump_;
-            cudaMemcpyAsync(d_inst_, &inst_, sizeof inst_, cudaMemcpyHostToDevice, C.st);
+            upload_inst(C.st);
         }
         launch_step_dt();
         JST_LAUNCH(K_.dump, sgrid(), K_.nt, K_.smem, C.st, d_tiles_, d_ntiles_, d_inst_, 0, RK_ALPHA[0]);
@@ -1023,8 +1058,7 @@ template <class T> class FusedEngine : public Engine {
         if (stage_ms) {
             cudaEventRecord(ev[2], st);
             for (int q = 0; q < 5; ++q) {
-                auto kern = q == 0 ? K_.stage[0] : (q == 4 ? K_.stage[2] : K_.stage[1]);
-                JST_LAUNCH(kern, sgrid(), K_.nt, K_.smem, st, d_tiles_, d_ntiles_, d_inst_, q, RK_ALPHA[q]);
+                launch_stage(q, st);
                 cudaEventRecord(ev[3 + q], st);
             }
         }

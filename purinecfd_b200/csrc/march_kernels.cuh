@@ -352,9 +352,13 @@ template <class T, int NT> constexpr int march_min_blocks() {
 // DUMP (with FIRST only): the residual R of every cell of the current state
 // goes to Inst::rdump instead of an update; nothing else is written and the
 // instance's step counters and stop flags are ignored.
-template <class T, int NT, bool FIRST, bool LAST, bool PIPE = false, bool DUMP = false, int STG = 0>
-__global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage,
-                                              double alpha) {
+// SOLO: every strip belongs to the one instance `solo` points to, a kernel
+// parameter (k_march_solo); its descriptor and constants are then read from
+// the parameter bank, as instruction operands, instead of being copied to
+// the warp's shared slot per strip and reloaded from global memory.
+template <class T, int NT, bool FIRST, bool LAST, bool PIPE, bool DUMP, int STG, bool SOLO>
+JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage, double alpha,
+                      const Inst<T>* solo) {
     using TD = typename std::conditional<LAST, double, T>::type;
     const int lane = JST_LANE();
     constexpr bool UR = march_u_ring<T>();
@@ -403,12 +407,21 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
         }
         if (dead) continue;
         const TileRef tr = tiles[ticket];
-        const Inst<T>& I = insts[tr.inst];
+        const Inst<T>* ip = insts + tr.inst;
+        if constexpr (SOLO) ip = solo;
+        const Inst<T>& I = *ip;
         const int ni = I.ni, nj = I.nj, i0 = tr.i0, j0 = tr.j0;
-        warp_copy_const(cwarp, &I.c);
-        if constexpr (sizeof(T) == sizeof(float)) warp_copy_const(kwarp, &I.cp);
-        const PhysConst& c = *cwarp;
-        const ConstP& K = *kwarp;
+        const PhysConst* cp = cwarp;
+        const ConstP* kp = kwarp;
+        if constexpr (SOLO) {
+            cp = &I.c;
+            kp = &I.cp;
+        } else {
+            warp_copy_const(cwarp, &I.c);
+            if constexpr (sizeof(T) == sizeof(float)) warp_copy_const(kwarp, &I.cp);
+        }
+        const PhysConst& c = *cp;
+        const ConstP& K = *kp;
 
         int hdr[3] = {0, 0, 0};  // skip, fresh, step
         if (lane == 0) {
@@ -1007,6 +1020,19 @@ __global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>())) k_march(const
             }
         }
     }
+}
+
+template <class T, int NT, bool FIRST, bool LAST, bool PIPE = false, bool DUMP = false, int STG = 0>
+__global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>()))
+    k_march(const TileRef* tiles, int* sched, const Inst<T>* insts, int stage, double alpha) {
+    march_body<T, NT, FIRST, LAST, PIPE, DUMP, STG, false>(tiles, sched, insts, stage, alpha, nullptr);
+}
+
+// The single-instance launch: the instance descriptor travels by value.
+template <class T, int NT, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NT, (march_min_blocks<T, NT>()))
+    k_march_solo(const TileRef* tiles, int* sched, int stage, double alpha, const __grid_constant__ Inst<T> solo) {
+    march_body<T, NT, FIRST, LAST, true, false, 0, true>(tiles, sched, nullptr, stage, alpha, &solo);
 }
 
 }  // namespace fused
