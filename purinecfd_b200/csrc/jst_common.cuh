@@ -355,10 +355,11 @@ JST_HD float fw_f32(float r, float cw2, float cw3_6, float one_plus_cw3_6, float
     return g > 1e5f ? fw_lim : v;
 }
 
-// source::compute for one cell (source.rs:55-85), before the factor V.
+// source::compute for one cell (source.rs:55-85), before the factor V,
+// given nu_tilde = rho_nu / rho (source.rs:62) as the caller has it.
 template <class T, bool Q = false>
-JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny, const PhysConst& c) {
-    T nu_tilde = dv<T, Q>(rho_nu, rho);
+JST_HD T sa_source_nt(T rho, T rho_nu, T nu_tilde, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny,
+                      const PhysConst& c) {
     T inv_kd2 = inv_dist2 * T(c.inv_kappa2);
     T ft2;
     if constexpr (sizeof(T) == sizeof(float)) ft2 = T(c.Ct3) * exp_f32(-T(c.Ct4) * chi * chi);
@@ -375,6 +376,11 @@ JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T 
     T destr = (T(c.cw1) * fw - T(c.cb1_k2) * ft2) * rho * (nu_tilde * nu_tilde * inv_dist2);
     T diff = T(c.cb2_sigma) * rho * (dnx * dnx + dny * dny);
     return prod - destr + diff;
+}
+
+template <class T, bool Q = false>
+JST_HD T sa_source(T rho, T rho_nu, T inv_dist2, T chi, T f1, T dvdx, T dudy, T dnx, T dny, const PhysConst& c) {
+    return sa_source_nt<T, Q>(rho, rho_nu, dv<T, Q>(rho_nu, rho), inv_dist2, chi, f1, dvdx, dudy, dnx, dny, c);
 }
 
 // boundary::extrapolate_nut (boundary.rs:158-185).  dist[k], nu[k] belong

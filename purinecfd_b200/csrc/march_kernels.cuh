@@ -305,6 +305,23 @@ template <class C> JST_D void warp_copy_const(C* dst, const C* src) {
 #endif
 }
 
+// Solver::unpack (solver.rs:158-181) for one cell of the marching kernels:
+// the temperature p / (R rho) is formed as p (1/rho) (1/R) from the
+// reciprocal the velocities already use and the strip's 1/R (two multiplies
+// instead of a quotient; within a few units in the last place of it).
+template <class T> JST_D Prim<T> unpack_cell_r(T u0, T u1, T u2, T u3, T u4, T gm1, T inv_rgas) {
+    Prim<T> q;
+    T inv = dv<T, true>(T(1), u0);
+    q.rho = u0;
+    q.vx = u1 * inv;
+    q.vy = u2 * inv;
+    q.e = u3 * inv;
+    q.p = gm1 * (u3 - u0 * (q.vx * q.vx + q.vy * q.vy) * T(0.5));
+    q.t = q.p * inv * inv_rgas;
+    q.nut = u4 * inv;
+    return q;
+}
+
 // A constant in the stage arithmetic: the FP32 copy for T = float, the FP64
 // value otherwise.
 template <class T> JST_D T kc(double d, float2 f) {
@@ -312,10 +329,9 @@ template <class T> JST_D T kc(double d, float2 f) {
     else return d;
 }
 
-// source::compute for one cell in FP32 (sa_source) from the FP32 constants.
-JST_D float sa_source_f32(float rho, float rho_nu, float inv_dist2, float chi, float f1, float dvdx, float dudy,
-                          float dnx, float dny, const ConstP& K) {
-    const float nu_tilde = dv<float, true>(rho_nu, rho);
+// source::compute for one cell in FP32 (sa_source_nt) from the FP32 constants.
+JST_D float sa_source_f32(float rho, float rho_nu, float nu_tilde, float inv_dist2, float chi, float f1, float dvdx,
+                          float dudy, float dnx, float dny, const ConstP& K) {
     const float inv_kd2 = inv_dist2 * K.inv_kappa2.x;
     const float ft2 = K.ct3.x * exp_f32(K.m_ct4.x * chi * chi);
     const float fv2 = 1.0f - dv<float, true>(chi, 1.0f + chi * f1);
@@ -461,6 +477,7 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
         const bool seam = cu < 0 || cu >= nj;
         const bool out_lane = lane >= 3 && lane < 3 + MARCH_W && cu < nj;
         const T gm1 = kc<T>(c.gm1, K.gm1), rgas = kc<T>(c.r_gas, K.r_gas);
+        const T inv_rgas = T(1) / rgas;  // once per strip
         const T half_cfl = kc<T>(c.half_cfl, K.half_cfl), k2 = kc<T>(c.k2, K.k2), k4 = kc<T>(c.k4, K.k4);
         // face fluxes are formed from twice the face state (see face_combine),
         // so the pressure reference of euler_flux is doubled as well
@@ -658,7 +675,7 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
                     p.e = kc<T>(c.f_e, K.f_e);
                     p.nut = kc<T>(c.f_nut, K.f_nut);
                 } else {
-                    p = unpack_cell<T, true>(uk[0], uk[1], uk[2], uk[3], uk[4], gm1, rgas);
+                    p = unpack_cell_r<T>(uk[0], uk[1], uk[2], uk[3], uk[4], gm1, inv_rgas);
                 }
                 if (seam) pack_cell<T>(p, uk);  // periodic ghost column (boundary.rs:54-72)
                 if (wall) {
@@ -762,10 +779,11 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
                     if (S || (r >= i0 && r < i1)) {
                         T s5;
                         if constexpr (sizeof(T) == sizeof(float))
-                            s5 = sa_source_f32(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7], K);
+                            s5 = sa_source_f32(UA(3, 0), UA(3, 4), qw[1][3], gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6],
+                                               g[7], K);
                         else
-                            s5 = sa_source<T, true>(UA(3, 0), UA(3, 4), gk[MG_D2], d.chi, d.fv1, g[2], g[1], g[6], g[7],
-                                                    c);
+                            s5 = sa_source_nt<T, true>(UA(3, 0), UA(3, 4), qw[1][3], gk[MG_D2], d.chi, d.fv1, g[2],
+                                                       g[1], g[6], g[7], c);
                         snew = s5 * gk[MG_VOL];
                     }
                     if (!S && r == 0) {
@@ -904,11 +922,11 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
                     Prim<double> q{};
                     if (sizeof(T) == sizeof(double)) {
                         double rho = un[0];
-                        q = unpack_cell<double, true>(un[0], un[1], un[2], un[3], un[4], c.gm1, c.r_gas);
+                        q = unpack_cell_r<double>(un[0], un[1], un[2], un[3], un[4], c.gm1, (double)inv_rgas);
                         bad = isnan(rho) || rho <= 1e-15 || isnan(q.p) || q.p <= 1e-15;
                     } else {
                         T rho = (T)un[0];
-                        Prim<T> qt = unpack_cell<T, true>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], gm1, rgas);
+                        Prim<T> qt = unpack_cell_r<T>(rho, (T)un[1], (T)un[2], (T)un[3], (T)un[4], gm1, inv_rgas);
                         bad = isnan(rho) || rho <= T(1e-15) || isnan(qt.p) || qt.p <= T(1e-15);
                         q.vx = qt.vx;
                         q.vy = qt.vy;
