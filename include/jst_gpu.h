@@ -225,8 +225,10 @@ jst_status jst_write_csv(jst_solver* s, const char* path);
 /* Device timing (no counterpart in the reference; used by benchmarks):
  * enqueues nsteps RK steps with the convergence test disabled and returns
  * their device time in *ms, measured with CUDA events on the solver's own
- * stream.  When stage_ms is non-NULL one further step is run stage by stage
- * and stage_ms[0..4] receive the five stage kernels' times. */
+ * stream.  When stage_ms is non-NULL ten further steps run back to back from
+ * one graph with a CUDA event recorded before, between and after each step's
+ * five stage launches, and stage_ms[0..4] receive the stage kernels' mean
+ * times over those steps. */
 jst_status jst_time_steps(jst_solver* s, int nsteps, double* ms, double* stage_ms);
 
 /* ------------------------------------------------------------------------

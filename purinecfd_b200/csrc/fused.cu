@@ -1037,7 +1037,11 @@ template <class T> class FusedEngine : public Engine {
     cudaStream_t stream() const override { return core_->st; }
 
     // nsteps graph-replayed steps with the target disabled, timed with CUDA
-    // events on the solver stream; optionally one more step stage by stage.
+    // events on the solver stream; optionally kStageReps more steps, run back
+    // to back from one graph with an event recorded before, between and
+    // after each step's stage launches, whose mean stage durations go to
+    // stage_ms.
+    static constexpr int kStageReps = 10;
     jst_status time_steps(int nsteps, double* ms, double* stage_ms) override {
         cudaStream_t st = core_->st;
         InstState s;
@@ -1046,33 +1050,55 @@ template <class T> class FusedEngine : public Engine {
         int zero = 0;
         cudaMemcpyAsync(&inst_.st->target, &never, sizeof never, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(&inst_.st->done, &zero, sizeof zero, cudaMemcpyHostToDevice, st);
-        int total = nsteps + (stage_ms ? 1 : 0);
+        int total = nsteps + (stage_ms ? kStageReps : 0);
         if ((size_t)(s.step + total) > hist_cap_) grow_hist((size_t)(s.step + total));
         set_max_step(s.step + total);
         ensure_graph();
-        cudaEvent_t ev[8];  // 0,1: around the steps; 2..7: stage boundaries of the extra step
+        cudaEvent_t ev[2 + 6 * kStageReps];  // 0,1: around the steps; then 6 per timed-stage step
         for (auto& e : ev) cudaEventCreate(&e);
         cudaEventRecord(ev[0], st);
         for (int q = 0; q < nsteps; ++q) launch_step();
         cudaEventRecord(ev[1], st);
-        if (stage_ms) {
-            cudaEventRecord(ev[2], st);
-            for (int q = 0; q < 5; ++q) {
-                launch_stage(q, st);
-                cudaEventRecord(ev[3 + q], st);
-            }
-        }
-        if (cudaEventSynchronize(stage_ms ? ev[7] : ev[1]) != cudaSuccess) return JST_ERR_CUDA;
+        jst_status rc = JST_OK;
+        if (cudaEventSynchronize(ev[1]) != cudaSuccess) rc = JST_ERR_CUDA;
         float t = 0.f;
         cudaEventElapsedTime(&t, ev[0], ev[1]);
         *ms = t;
-        if (stage_ms)
-            for (int q = 0; q < 5; ++q) {
-                float tq = 0.f;
-                cudaEventElapsedTime(&tq, ev[2 + q], ev[3 + q]);
-                stage_ms[q] = tq;
+        if (stage_ms && rc == JST_OK) {
+            cudaGraph_t g;
+            cudaGraphExec_t tg = nullptr;
+            cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            for (int r = 0; r < kStageReps; ++r) {
+                cudaEvent_t* e = ev + 2 + 6 * r;
+                cudaEventRecordWithFlags(e[0], st, cudaEventRecordExternal);
+                for (int q = 0; q < 5; ++q) {
+                    launch_stage(q, st);
+                    cudaEventRecordWithFlags(e[1 + q], st, cudaEventRecordExternal);
+                }
             }
+            if (cudaStreamEndCapture(st, &g) != cudaSuccess) {
+                rc = JST_ERR_CUDA;
+            } else {
+                if (cudaGraphInstantiate(&tg, g, 0) != cudaSuccess) rc = JST_ERR_CUDA;
+                cudaGraphDestroy(g);
+            }
+            if (rc == JST_OK) {
+                cudaGraphLaunch(tg, st);
+                if (cudaEventSynchronize(ev[1 + 6 * kStageReps]) != cudaSuccess) rc = JST_ERR_CUDA;
+            }
+            if (tg) cudaGraphExecDestroy(tg);
+            for (int q = 0; q < 5 && rc == JST_OK; ++q) {
+                double acc = 0.0;
+                for (int r = 0; r < kStageReps; ++r) {
+                    float tq = 0.f;
+                    cudaEventElapsedTime(&tq, ev[2 + 6 * r + q], ev[3 + 6 * r + q]);
+                    acc += tq;
+                }
+                stage_ms[q] = acc / kStageReps;
+            }
+        }
         for (auto& e : ev) cudaEventDestroy(e);
+        if (rc != JST_OK) return rc;
         cudaMemcpyAsync(&inst_.st->target, &core_->targetres, sizeof(double), cudaMemcpyHostToDevice, st);
         if (read_state(&s) != JST_OK) return JST_ERR_CUDA;
         if (s.err) return JST_ERR_TIMEOUT;
