@@ -859,12 +859,31 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
                     T e4 = tmax<T>(k4 - e2, T(0));
                     T lam = half_cfl * (rt0 + jst_shfl_up(rt0, 1));
                     T ul1[5], ul2[5], ur1[5], fu[5], cv[5], um[5];
-                    for (int v = 0; v < 5; ++v) {
-                        um[v] = UA(1, v);
-                        ul1[v] = jst_shfl_up(um[v], 1);
-                        ul2[v] = jst_shfl_up(um[v], 2);
-                        ur1[v] = jst_shfl_down(um[v], 1);
-                        fu[v] = ul1[v] + um[v];
+                    if constexpr (UR) {
+                        // the neighbours' U of row m from the ring (one shared
+                        // load each instead of two shuffles of the halves);
+                        // lanes 0-2 and 31, whose faces are not used, clamp
+                        __syncwarp();  // ring rows written by other lanes
+                        int sl = s0 + 2;
+                        sl = sl >= 5 ? sl - 5 : sl;
+                        const int l1 = lane > 0 ? lane - 1 : 0, l2 = lane > 1 ? lane - 2 : 0;
+                        const int r1 = lane < 31 ? lane + 1 : 31;
+                        for (int v = 0; v < 5; ++v) {
+                            const T* ur = uring->u[sl][v];
+                            um[v] = ur[lane];
+                            ul1[v] = ur[l1];
+                            ul2[v] = ur[l2];
+                            ur1[v] = ur[r1];
+                            fu[v] = ul1[v] + um[v];
+                        }
+                    } else {
+                        for (int v = 0; v < 5; ++v) {
+                            um[v] = UA(1, v);
+                            ul1[v] = jst_shfl_up(um[v], 1);
+                            ul2[v] = jst_shfl_up(um[v], 2);
+                            ur1[v] = jst_shfl_down(um[v], 1);
+                            fu[v] = ul1[v] + um[v];
+                        }
                     }
                     euler_flux<T, true>(fu, nx2[0], ny2[0], gm1, cv, p_ref2);
                     T hx = T(0.5) * nx2[0], hy = T(0.5) * ny2[0];
