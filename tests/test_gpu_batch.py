@@ -107,3 +107,26 @@ def test_kernel_configuration_is_reported():
     tuned.run_all(chunk=10)
     ti, tj, nt = tuned.kernel_config()
     assert tj in (26, 32, 64) and ti > 0 and nt in (64, 128, 256)
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "split"])
+def test_single_instance_kernel_equals_batch_kernel(prec):
+    """A single solve on marching strips runs the kernel that takes the
+    instance descriptor as a parameter (k_march_solo); a batch runs the one
+    that reads it from the instance table.  Same strips, same arithmetic: the
+    states agree bit for bit."""
+    from purinecfd_b200 import DT_LOCAL, Solver
+    from purinecfd_b200.batch import Batch
+    cfg, xy, nr, nt = _cases()[2]
+    steps = 40
+    s = Solver(cfg, xy, nr, nt, precision=prec, dt_mode=DT_LOCAL, tile_i=16, tile_j=26, block_threads=64)
+    s.run(steps)
+    b = Batch(precision=prec, dt_mode=DT_LOCAL, steps_per_poll=20, keep_fields=True, hbm_budget_gb=1.0, tile_i=16,
+              tile_j=26, block_threads=64)
+    b.submit(cfg, xy, nr, nt, max_steps=steps)
+    r = b.run_all(chunk=20)[0]
+    assert s.kernel_config() == b.kernel_config() == (16, 26, 64)
+    for c in range(5):
+        assert np.array_equal(s.get(f"U{c}"), r.fields[c]), c
+    s.close()
+    b.close()
