@@ -383,6 +383,10 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
     // from rounding U_n - increment once by at most one FP32 rounding); the
     // last stage adds its increment to U_n in FP64.
     constexpr bool ACC32 = sizeof(T) == sizeof(float) && !LAST;
+    // FP64, stage 0: the stage input is U_n itself, so the accumulator of the
+    // updated row is the U ring's copy of it (the value loaded three rows
+    // earlier) instead of a second load
+    constexpr bool UN_RING = FIRST && sizeof(T) == sizeof(double) && march_u_ring<T>();
     using RowT = typename std::conditional<STG == 1, MarchRowB<T>, MarchRow<T>>::type;
     RowT* rowbuf = nullptr;
     MarchURing<T>* uring = nullptr;
@@ -531,7 +535,7 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
                         if constexpr (ACC32) {
                             if constexpr (!FIRST)
                                 for (int v = 0; v < 5; ++v) seg(B.uacc[v], I.uc[0] + v * np + mr, (int)sizeof(T), sT, WT);
-                        } else {
+                        } else if constexpr (!UN_RING) {
                             for (int v = 0; v < 5; ++v) seg(B.un[v], I.un[0] + v * np + mr, 8, sD, WD);
                         }
                         if (dt_local) seg(B.ldt, I.ldt + mr, 8, sD, WD);
@@ -577,7 +581,7 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
                 if constexpr (ACC32) {
                     if constexpr (!FIRST)  // stage 0 reads the same values as its stage input
                         for (int v = 0; v < 5; ++v) async_copy<sizeof(T)>(&B.uacc[v][lane], I.uc[0] + v * np + id);
-                } else {
+                } else if constexpr (!UN_RING) {
                     for (int v = 0; v < 5; ++v) async_copy<8>(&B.un[v][lane], I.un[0] + v * np + id);
                 }
                 if (dt_local) async_copy<8>(&B.ldt[lane], I.ldt + id);
@@ -926,7 +930,9 @@ JST_D void march_body(const TileRef* tiles, int* sched, const Inst<T>* insts, in
                             un[v] = (double)nv;
                             if (out_lane) dst[v * np + id] = (TD)nv;
                         } else {
-                            double uo = PIPE ? B->un[v][oD + lane] : I.un[0][v * np + id];
+                            double uo;
+                            if constexpr (UN_RING) uo = (double)UA(1, v);
+                            else uo = PIPE ? B->un[v][oD + lane] : I.un[0][v * np + id];
                             if (v == 0) uo0 = uo;
                             if (sizeof(T) == sizeof(double)) un[v] = uo - (double)R[v] * sc;
                             else un[v] = uo - (double)(R[v] * (T)sc);  // FP32 increment, FP64 accumulator
