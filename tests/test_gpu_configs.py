@@ -51,14 +51,23 @@ def reference(request):
     return name, steps, cfg, (xy, nr, nt), {"residual": res, "fields": fields, "cl": cl, "cd": cd}
 
 
-@pytest.mark.parametrize("path", ["fused_fp64", "passes", "fused_split"])
+# the *_strips paths force the marching strips, whose single-solve kernel takes
+# the instance descriptor as a launch parameter: the 5000-step run outgrows the
+# residual history (4096 steps), and the step graph is captured again after it
+STRIPS = dict(tile_i=16, tile_j=26, block_threads=64)
+
+
+@pytest.mark.parametrize("path", ["fused_fp64", "passes", "fused_split", "fused_fp64_strips", "fused_split_strips"])
 def test_full_run_matches_oracle(reference, path):
     from purinecfd_b200 import PATH_FUSED, PATH_PASSES, PREC_FP32_SPLIT, PREC_FP64, Solver
     name, steps, cfg, (xy, nr, nt), ref = reference
     kw = {"fused_fp64": dict(kernel_path=PATH_FUSED, precision=PREC_FP64),
           "passes": dict(kernel_path=PATH_PASSES, precision=PREC_FP64),
-          "fused_split": dict(kernel_path=PATH_FUSED, precision=PREC_FP32_SPLIT)}[path]
-    field_tol, force_tol = (1e-4, 1e-4) if path == "fused_split" else (1e-10, 1e-8)
+          "fused_split": dict(kernel_path=PATH_FUSED, precision=PREC_FP32_SPLIT),
+          "fused_fp64_strips": dict(kernel_path=PATH_FUSED, precision=PREC_FP64, **STRIPS),
+          "fused_split_strips": dict(kernel_path=PATH_FUSED, precision=PREC_FP32_SPLIT, **STRIPS)}[path]
+    split = path.startswith("fused_split")
+    field_tol, force_tol = (1e-4, 1e-4) if split else (1e-10, 1e-8)
     s = Solver(cfg, xy, nr, nt, **kw)
     rep = s.run(steps)
     assert rep.steps == steps
@@ -66,6 +75,11 @@ def test_full_run_matches_oracle(reference, path):
         assert rel_field_err(s.get(f), ref["fields"][f]) < field_tol, (name, f)
     cl, cd = s.forces()
     assert abs(cl - ref["cl"]) < force_tol and abs(cd - ref["cd"]) < force_tol, (cl, ref["cl"], cd, ref["cd"])
-    if path != "fused_split":
+    if not split:
         assert abs(rep.residual - ref["residual"]) < 1e-10 * ref["residual"]
+    if "strips" in path:
+        assert s.kernel_config() == (16, 26, 64)
+        hist = []
+        s.run(3, lambda k, r: hist.append(r))  # after the history grew: the graph runs on
+        assert len(hist) == 3 and all(np.isfinite(hist))
     s.close()
