@@ -128,6 +128,90 @@ void nonphysical_report(const PhysConst& c, long i, long j, const double u[5], j
 }
 
 // ------------------------------------------------------- passes engine ----
+// Touches every page of a large output buffer from several threads before a
+// device-to-host copy into it.  A freshly allocated host array is mapped on
+// first write, and the kernel zero-fills each new page on the faulting
+// thread; done inside the copy that runs on one thread at a few GB/s (on a
+// 4.2 M-cell field, 9 ms of a copy that takes 2 ms into mapped memory).
+// Each touch writes back the byte it read, so the caller's data is unchanged
+// when the call then fails.
+static void prefault(void* p, size_t bytes) {
+    constexpr size_t kPage = 4096, kMin = size_t(4) << 20;
+    if (bytes < kMin) return;
+    const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t per = (bytes + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t)
+        th.emplace_back([=] {
+            volatile char* c = static_cast<volatile char*>(p);
+            const size_t a = t * per, b = std::min(bytes, a + per);
+            for (size_t k = a; k < b; k += kPage) c[k] = c[k];
+        });
+    for (auto& x : th) x.join();
+}
+
+// Copies n bytes from src to dst with up to 8 host threads, each on its own
+// page-aligned range (a fresh destination is mapped by the threads in
+// parallel).
+static void parallel_copy(void* dst, const void* src, size_t n) {
+    constexpr size_t kPage = 4096;
+    const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t per = ((n + nt - 1) / nt + kPage - 1) / kPage * kPage;
+    std::vector<std::thread> th;
+    for (size_t a = 0; a < n; a += per) {
+        const size_t b = std::min(n, a + per);
+        th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
+    }
+    for (auto& x : th) x.join();
+}
+
+// A device-to-host copy into pageable memory runs through the driver's own
+// staging at a few GB/s on one thread.  Reads of 4 MiB and more go instead
+// through two pinned 8 MiB buffers of the solver (allocated on first use,
+// freed with the solver): the device fills one at full link rate while
+// parallel_copy moves the other on.  If the pinned buffers cannot be had,
+// the plain copy is used.
+cudaError_t d2h_staged(SolverCore& C, void* dst, const void* src, size_t bytes) {
+    constexpr size_t kMin = size_t(4) << 20, kChunk = size_t(8) << 20;
+    if (bytes >= kMin && !C.pin) {
+        if (cudaHostAlloc(&C.pin, 2 * kChunk, cudaHostAllocDefault) == cudaSuccess) {
+            C.pin_bytes = 2 * kChunk;
+        } else {
+            C.pin = nullptr;
+            cudaGetLastError();
+        }
+    }
+    if (bytes < kMin || !C.pin) {
+        prefault(dst, bytes);
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, C.st);
+        return e != cudaSuccess ? e : cudaStreamSynchronize(C.st);
+    }
+    char* buf[2] = {static_cast<char*>(C.pin), static_cast<char*>(C.pin) + kChunk};
+    cudaEvent_t ev[2];
+    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    const size_t nch = (bytes + kChunk - 1) / kChunk;
+    auto issue = [&](size_t q) {
+        const size_t off = q * kChunk, n = std::min(kChunk, bytes - off);
+        cudaError_t e = cudaMemcpyAsync(buf[q & 1], static_cast<const char*>(src) + off, n, cudaMemcpyDeviceToHost,
+                                        C.st);
+        return e == cudaSuccess ? cudaEventRecord(ev[q & 1], C.st) : e;
+    };
+    cudaError_t e = issue(0);
+    for (size_t q = 0; q < nch && e == cudaSuccess; ++q) {
+        if (q + 1 < nch) e = issue(q + 1);  // its buffer was emptied by chunk q-1's copy
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[q & 1]);
+        if (e == cudaSuccess) {
+            const size_t off = q * kChunk;
+            parallel_copy(static_cast<char*>(dst) + off, buf[q & 1], std::min(kChunk, bytes - off));
+        }
+    }
+    if (e != cudaSuccess) cudaStreamSynchronize(C.st);  // no copy into the buffers stays in flight
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return e;
+}
+
 class PassesEngine : public Engine {
   public:
     PassesEngine(SolverCore* core) : core_(core) {}
@@ -209,6 +293,7 @@ class PassesEngine : public Engine {
         const double* base;
         int stride, h;
         if (!passes_field(P_, id, &base, &stride, &h)) return false;
+        prefault(out, sizeof(double) * core_->ni * core_->nj);
         cudaMemcpy2DAsync(out, sizeof(double) * core_->nj, base + (size_t)h * stride + h, sizeof(double) * stride,
                           sizeof(double) * core_->nj, core_->ni, cudaMemcpyDeviceToHost, core_->st);
         return cudaStreamSynchronize(core_->st) == cudaSuccess;
@@ -288,6 +373,7 @@ struct jst_solver {
         if (core.geom_arena) cudaFree(core.geom_arena);
         if (core.d_xy) cudaFree(core.d_xy);
         if (core.d_scratch) cudaFree(core.d_scratch);
+        if (core.pin) cudaFreeHost(core.pin);
         if (core.st) cudaStreamDestroy(core.st);
     }
 };
@@ -556,33 +642,10 @@ jst_status jst_step_count(const jst_solver* s, int64_t* out) {
     return JST_OK;
 }
 
-// Touches every page of a large output buffer from several threads before a
-// device-to-host copy into it.  A freshly allocated host array is mapped on
-// first write, and the kernel zero-fills each new page on the faulting
-// thread; done inside the copy that runs on one thread at a few GB/s (on a
-// 4.2 M-cell field, 9 ms of a copy that takes 2 ms into mapped memory).
-// Each touch writes back the byte it read, so the caller's data is unchanged
-// when the call then fails.
-static void prefault(void* p, size_t bytes) {
-    constexpr size_t kPage = 4096, kMin = size_t(4) << 20;
-    if (bytes < kMin) return;
-    const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-    const size_t per = (bytes + nt - 1) / nt;
-    std::vector<std::thread> th;
-    for (unsigned t = 0; t < nt; ++t)
-        th.emplace_back([=] {
-            volatile char* c = static_cast<volatile char*>(p);
-            const size_t a = t * per, b = std::min(bytes, a + per);
-            for (size_t k = a; k < b; k += kPage) c[k] = c[k];
-        });
-    for (auto& x : th) x.join();
-}
-
 jst_status jst_get_field(jst_solver* s, int field, double* out, size_t n) {
     if (!s || !out || field < 0 || field >= JST_F_COUNT) return JST_ERR_ARG;
     size_t nc = (size_t)s->core.ni * s->core.nj;
     if (n < nc) return JST_ERR_ARG;
-    prefault(out, nc * sizeof(double));
     const Geom& g = s->core.g;
     const double* geo = nullptr;
     switch (field) {
@@ -593,8 +656,7 @@ jst_status jst_get_field(jst_solver* s, int field, double* out, size_t n) {
         default: break;
     }
     if (geo) {
-        if (cudaMemcpy(out, geo, nc * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
-            return cuda_fail(s, "get_field");
+        if (d2h_staged(s->core, out, geo, nc * sizeof(double)) != cudaSuccess) return cuda_fail(s, "get_field");
         return JST_OK;
     }
     if (!s->eng->get_field(field, out)) {

@@ -950,14 +950,9 @@ template <class T> class FusedEngine : public Engine {
     bool get_field(int id, double* out) override {
         SolverCore& C = *core_;
         size_t n = (size_t)C.ni * C.nj;
-        if (id == JST_F_LOCALDT && C.local_dt) {
-            return cudaMemcpy(out, inst_.ldt, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess;
-        }
+        if (id == JST_F_LOCALDT && C.local_dt) return d2h_staged(C, out, inst_.ldt, n * sizeof(double)) == cudaSuccess;
         if (id > JST_F_U4) return false;
-        if (id >= JST_F_U0) {
-            return cudaMemcpy(out, inst_.un[id - JST_F_U0], n * sizeof(double), cudaMemcpyDeviceToHost) ==
-                   cudaSuccess;
-        }
+        if (id >= JST_F_U0) return d2h_staged(C, out, inst_.un[id - JST_F_U0], n * sizeof(double)) == cudaSuccess;
         InstState s;
         if (read_state(&s) != JST_OK) return false;
         const PhysConst& c = C.c;
@@ -969,8 +964,7 @@ template <class T> class FusedEngine : public Engine {
         UnPtrs up;
         for (int k = 0; k < 5; ++k) up.u[k] = inst_.un[k];
         JST_LAUNCH(k_prim_field, (unsigned)((n + 255) / 256), 256, 0, core_->st, up, (long)n, id, c, d_field_);
-        return cudaMemcpyAsync(out, d_field_, n * sizeof(double), cudaMemcpyDeviceToHost, core_->st) == cudaSuccess &&
-               cudaStreamSynchronize(core_->st) == cudaSuccess;
+        return d2h_staged(C, out, d_field_, n * sizeof(double)) == cudaSuccess;
     }
 
     jst_status set_conserved(const double* u5, jst_nonphysical* bad) override {
