@@ -319,7 +319,8 @@ std::vector<TileRef> make_tiles(int inst, int ni, int nj, int ti, int tj) {
     int a_n = (ni + ti - 1) / ti, b_n = (nj + tj - 1) / tj;
     t.reserve((size_t)a_n * b_n);
     for (int a = 0; a < a_n; ++a) {
-        // marching strips: a_n bands of nearly equal height (at most ti rows)
+        // marching strips: a_n bands of nearly equal height, at most ti rows
+        // (k_step_dt walks TI rows of each work item)
         int i0 = strip_width(tj) ? (int)((long)a * ni / a_n) : a * ti;
         int i1 = strip_width(tj) ? (int)((long)(a + 1) * ni / a_n) : std::min(a * ti + ti, ni);
         for (int b = 0; b < b_n; ++b) t.push_back(TileRef{inst, i0, b * tj, a * b_n + b, i1});
