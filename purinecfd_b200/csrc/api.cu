@@ -15,6 +15,7 @@
 #include <fstream>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <thread>
@@ -167,26 +168,32 @@ static void parallel_copy(void* dst, const void* src, size_t n) {
 
 // A device-to-host copy into pageable memory runs through the driver's own
 // staging at a few GB/s on one thread.  Reads of 4 MiB and more go instead
-// through two pinned 8 MiB buffers of the solver (allocated on first use,
-// freed with the solver): the device fills one at full link rate while
-// parallel_copy moves the other on.  If the pinned buffers cannot be had,
+// through two pinned 8 MiB buffers: the device fills one at full link rate
+// while parallel_copy moves the other on.  The buffers belong to the process
+// (portable pinned memory, valid for every device; allocated by the first
+// large read, about 10 ms, and kept until exit) and are taken under a mutex,
+// so concurrent reads of several solvers take turns.  If they cannot be had,
 // the plain copy is used.
+static std::mutex g_pin_mu;
+static char* g_pin = nullptr;
+
 cudaError_t d2h_staged(SolverCore& C, void* dst, const void* src, size_t bytes) {
     constexpr size_t kMin = size_t(4) << 20, kChunk = size_t(8) << 20;
-    if (bytes >= kMin && !C.pin) {
-        if (cudaHostAlloc(&C.pin, 2 * kChunk, cudaHostAllocDefault) == cudaSuccess) {
-            C.pin_bytes = 2 * kChunk;
-        } else {
-            C.pin = nullptr;
-            cudaGetLastError();
+    std::unique_lock<std::mutex> lk(g_pin_mu, std::defer_lock);
+    if (bytes >= kMin) {
+        lk.lock();
+        if (!g_pin) {
+            void* p = nullptr;
+            if (cudaHostAlloc(&p, 2 * kChunk, cudaHostAllocPortable) == cudaSuccess) g_pin = static_cast<char*>(p);
+            else cudaGetLastError();
         }
     }
-    if (bytes < kMin || !C.pin) {
+    if (bytes < kMin || !g_pin) {
         prefault(dst, bytes);
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, C.st);
         return e != cudaSuccess ? e : cudaStreamSynchronize(C.st);
     }
-    char* buf[2] = {static_cast<char*>(C.pin), static_cast<char*>(C.pin) + kChunk};
+    char* buf[2] = {g_pin, g_pin + kChunk};
     cudaEvent_t ev[2];
     cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
@@ -373,7 +380,6 @@ struct jst_solver {
         if (core.geom_arena) cudaFree(core.geom_arena);
         if (core.d_xy) cudaFree(core.d_xy);
         if (core.d_scratch) cudaFree(core.d_scratch);
-        if (core.pin) cudaFreeHost(core.pin);
         if (core.st) cudaStreamDestroy(core.st);
     }
 };

@@ -29,12 +29,10 @@ struct SolverCore {
     double* geom_arena = nullptr;
     double* d_xy = nullptr;
     double* d_scratch = nullptr;
-    void* pin = nullptr;  // pinned staging buffer of large device-to-host reads (d2h_staged)
-    size_t pin_bytes = 0;
 };
 
 // Device-to-host copy of `bytes` on the solver's stream into pageable host
-// memory, through the solver's pinned staging buffer for large reads.
+// memory, through the process's pinned staging buffers for large reads.
 cudaError_t d2h_staged(SolverCore& C, void* dst, const void* src, size_t bytes);
 
 void nonphysical_report(const PhysConst& c, long i, long j, const double u[5], jst_nonphysical* bad);
