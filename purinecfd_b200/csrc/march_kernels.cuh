@@ -7,8 +7,9 @@
 // j0-3+L (a 3-column halo on each side), so every j-neighbour the stencil
 // needs is one or two lanes away and comes from a register shuffle; the warp
 // walks down the rows i0-3 .. i1+2 keeping sliding windows of the rows it
-// still needs in registers (U: 4 rows, primitives: 2, sensors: 3, diffusion
-// tensors: 2, the previous tau-face flux).  Every value is loaded from HBM
+// still needs in registers (U: 4 rows, in FP64 a per-warp shared ring;
+// primitives: 2, sensors: 3, diffusion tensors: 2, the previous tau-face
+// flux).  Every value is loaded from HBM
 // once per strip and computed once per cell (plus a 6-row warm-up and the
 // 6-lane halo), no block barrier is used, and warps take strips from a
 // per-launch work counter so uneven instances balance.
@@ -18,7 +19,11 @@
 //   gradients + diffusion tensor + SA source of row k-1;
 //   tau face k-2;  n faces of row k-3 and the RK update of row k-3.
 // The arithmetic of every term is the one k_stage uses (shared helpers in
-// jst_common.cuh), in the same operation order.
+// jst_common.cuh), in the same operation order, except two quotients: the
+// temperature comes from the cell's reciprocal density and 1/R
+// (unpack_cell_r), the SA source takes nu-tilde from the primitive window.
+// A single solve launches the walk as k_march_solo (the instance descriptor a
+// kernel parameter), a batch as k_march.
 #pragma once
 
 #ifndef JST_LANE
